@@ -1,0 +1,105 @@
+"""Named workloads: camera/state records (C, 64 floats) and input records
+(I, 32 floats) for the measured configurations.  Pure numpy; every
+implementation (GPU library, CPU oracle, reference harness build) is fed the
+same arrays.
+
+Field maps follow the reference: C (Arbor.cu:179-182, 51, 277-304) and
+I (Arbor.cu:182).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+FOREST_SEED = 7
+TREE_SEED = 1
+
+
+def hash_u(x: int) -> int:
+    """The reference's integer hash (Arbor.cu:32)."""
+    x &= 0xFFFFFFFF
+    x ^= x >> 16
+    x = (x * 2146121005) & 0xFFFFFFFF
+    x ^= x >> 15
+    x = (x * 2221713035) & 0xFFFFFFFF
+    x ^= x >> 16
+    return x
+
+
+def rnd(n: int, seed: int) -> float:
+    """Arbor.cu:33 - float32 value of the 24-bit hash fraction."""
+    h = hash_u((n & 0xFFFFFFFF) ^ hash_u(seed & 0xFFFFFFFF))
+    return float(np.float32(h & 16777215) / np.float32(16777216.0))
+
+
+def base_state(seed: int, width: int, height: int) -> np.ndarray:
+    """initCamera's defaults (Arbor.cu:181) without the pose."""
+    C = np.zeros(64, np.float32)
+    C[12] = -0.45
+    C[13] = 0.63
+    C[14] = 0.90
+    C[20] = 1.18
+    C[22] = 1.0
+    C[23] = 1.0
+    C[31] = seed
+    C[44] = 1.0
+    C[3] = 1.0
+    C[18] = 1.0
+    C[32] = width
+    C[33] = height
+    return C
+
+
+def single_tree_camera(width: int = 256, height: int = 256, seed: int = TREE_SEED) -> np.ndarray:
+    """One tree, first-person camera at 1.72 m eye height, 6 m from the
+    trunk, 60 degree vertical field of view, looking at the crown centre
+    (0, 5.4, 0); shadows off, lit view mode, first sample with history reset.
+
+    cameraRay (Arbor.cu:51) spans v in [-0.5, 0.5] * C[14], so a 60 degree
+    vertical FOV is C[14] = 2 tan(30 deg).
+    """
+    C = base_state(seed, width, height)
+    C[0:3] = (0.0, 1.72, 6.0)
+    C[4:7] = (0.0, 5.4, 0.0)
+    C[14] = np.float32(2.0 * math.tan(math.radians(30.0)))
+    C[16] = math.pi
+    C[17] = math.atan2(5.4 - 1.72, 6.0)
+    C[22] = 0.0
+    C[15] = 0.0
+    C[9] = 0.0
+    C[10] = 1.0
+    return C
+
+
+def walk_input(frame: int, seed: int = FOREST_SEED) -> tuple[np.ndarray, float]:
+    """Input record and dt of frame `frame` of the seeded forest walk.
+
+    The walk uses the reference's own camera state machine (updateCamera,
+    Arbor.cu:182): forward key held (I[15] = 1) and a mouse turn
+    I[0] = (rnd(frame, seed) - 0.5) * 20 (a heading random walk of at most
+    +-0.0225 rad per frame).  updateCamera walks at 4.2 m/s of `delta`, so
+    delta = 1/180 s advances 4.2/180 m per frame: 1.4 m/s at 60 frames/s.
+    Eye height is pinned to 1.72 m by updateCamera.
+    """
+    I = np.zeros(32, np.float32)
+    I[0] = (rnd(frame, seed) - 0.5) * 20.0
+    I[15] = 1.0
+    return I, 1.0 / 180.0
+
+
+def forest_start_state(width: int = 1920, height: int = 1080, seed: int = FOREST_SEED, shadows: bool = False) -> np.ndarray:
+    """Walk start: initCamera's preset-1 pose (eye (2, 1.72, 18), yaw pi) is
+    applied by running initCamera itself; this returns the fields the walk
+    changes on top of it."""
+    C = base_state(seed, width, height)
+    C[22] = 1.0 if shadows else 0.0
+    return C
+
+
+def shadow_sun(seed: int = FOREST_SEED) -> tuple[float, float]:
+    """Sun azimuth from the seed and 35 degree elevation (C[12], C[13])."""
+    return 2.0 * math.pi * rnd(0, seed), math.radians(35.0)
+
+
+VIEW_PRESETS = (1, 2, 3, 4, 5)

@@ -1,0 +1,233 @@
+/*
+ * arbor.h - C ABI of the B200-native Arbor render path.
+ *
+ * Drop-in for the reference's 12 kernel entry points.  Each entry keeps the
+ * buffer order, element types and scalars of the reference's kernel metadata
+ * (generated/<entry>.json "bindings"/"scalars", generated/manifest.json) and
+ * the reference kernel's semantics (Arbor.cu, cited per entry).  The engine
+ * (src/engine.js:26-53) bound buffers and dispatched workgroups through
+ * Kernel.bind + ComputeBatch.dispatch (vendor/cuda-webshader/runtime/
+ * runtime.js:279,347); here the caller passes device pointers and a CUDA
+ * stream, and the callee derives the grid.
+ *
+ * Conventions
+ *  - All buffers are caller-owned device memory with the ABI sizes below.
+ *    Entry points never allocate or free caller buffers.
+ *  - Every entry returns an arbor_status (0 = ARBOR_OK).  No exception or
+ *    abort crosses the ABI.  arbor_last_error() gives a message for the
+ *    calling thread's most recent failure.
+ *  - Calls on one stream execute in issue order, as the reference's
+ *    dispatches inside one pass do (docs/ARCHITECTURE.md:19).
+ *  - Argument checks mirror runtime.js: non-finite scalars
+ *    (runtime.js:18-22), writable aliasing across bindings (runtime.js:325),
+ *    workgroup counts above 65535 (runtime.js:352); plus null and
+ *    misaligned pointers, which a WebGPU binding cannot express.
+ *  - A launch error is reported as ARBOR_ERR_CUDA; the kernel itself runs
+ *    asynchronously on `stream`.
+ */
+#ifndef ARBOR_H
+#define ARBOR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ARBOR_API __attribute__((visibility("default")))
+#else
+#define ARBOR_API
+#endif
+
+/* Same type as cudaStream_t; NULL is the legacy default stream. */
+typedef struct CUstream_st* arbor_stream;
+
+/* ABI constants (kernels/common.cu:2-12, src/engine.js:2). */
+#define ARBOR_CAPACITY 32768
+#define ARBOR_NODE_COUNT 65536
+#define ARBOR_PS 24
+#define ARBOR_CS 20
+#define ARBOR_CURVES 2109
+#define ARBOR_WOOD_COUNT 5124
+#define ARBOR_LEAF_COUNT 24192
+#define ARBOR_ROCK_COUNT 96
+#define ARBOR_OBJECT_COUNT 29412
+#define ARBOR_FOREST_SIDE 18
+#define ARBOR_FOREST_COUNT 324
+
+/* Buffer sizes in elements (src/engine.js:22,40). */
+#define ARBOR_B_FLOATS (ARBOR_CURVES * ARBOR_CS)
+#define ARBOR_P_FLOATS (ARBOR_CAPACITY * ARBOR_PS)
+#define ARBOR_NODES_FLOATS (ARBOR_NODE_COUNT * 8)
+#define ARBOR_C_FLOATS 64
+#define ARBOR_I_FLOATS 32
+/* Hit, Linear, Guide, Filtered, History: width*height*4 floats.
+ * Pixels: width*height uint32 (RGBA8, R in the low byte). */
+
+typedef enum arbor_status {
+  ARBOR_OK = 0,
+  ARBOR_ERR_NULL = 1,          /* a required pointer is NULL */
+  ARBOR_ERR_VALUE = 2,         /* a scalar is non-finite or out of range */
+  ARBOR_ERR_ALIGN = 3,         /* a buffer is not 16-byte aligned */
+  ARBOR_ERR_ALIAS = 4,         /* a writable buffer overlaps another binding */
+  ARBOR_ERR_LIMIT = 5,         /* grid above 65535 workgroups per dimension, or
+                                  a size above a stated maximum */
+  ARBOR_ERR_CUDA = 6,          /* a CUDA runtime call failed */
+  ARBOR_ERR_TIMEOUT = 7,       /* a bounded device wait gave up */
+  ARBOR_ERR_STATE = 8,         /* object disposed or in the wrong state */
+  ARBOR_ERR_NO_DEVICE = 9      /* no CUDA device is available */
+} arbor_status;
+
+/* Message for the calling thread's last failing call ("" if none). */
+ARBOR_API const char* arbor_last_error(void);
+/* Human-readable name of a status code. */
+ARBOR_API const char* arbor_status_name(int status);
+/* 1 when this library was built for sm_100a and a device is present. */
+ARBOR_API int arbor_device_ready(void);
+/* Number of kernels this library has launched in this process (all entries,
+ * all threads).  Tests and the benchmark use it to count launches. */
+ARBOR_API uint64_t arbor_launch_count(void);
+
+/* ---------------------------------------------------------------------------
+ * The 12 reference entry points.
+ * ------------------------------------------------------------------------- */
+
+/* One generation of branch curves into B (Arbor.cu:76-102; bindings B rw;
+ * scalars level, seed).  Levels 0..4 launch 9/12/72/288/1728 threads as the
+ * harness does (tests/native_harness.cpp:45); any other level runs the level-4
+ * thread count with the reference kernel's fall-through semantics. */
+ARBOR_API int arbor_growTree(float* B, int level, int seed, arbor_stream stream);
+
+/* 32768 primitive records (Arbor.cu:103-131; bindings B r, P w; scalar seed). */
+ARBOR_API int arbor_makePrimitives(const float* B, float* P, int seed, arbor_stream stream);
+
+/* 30-bit Morton key per primitive centroid and identity order
+ * (Arbor.cu:138-139; bindings P r, Keys w, Order w). */
+ARBOR_API int arbor_makeKeys(const float* P, uint32_t* Keys, uint32_t* Order, arbor_stream stream);
+
+/* One bitonic compare-exchange stage over (key, index) (Arbor.cu:140;
+ * bindings Keys rw, Order rw; scalars distance, span).  distance must lie in
+ * 0..32767 (a larger one indexes past the 32768 records). */
+ARBOR_API int arbor_sortPass(uint32_t* Keys, uint32_t* Order, int distance, int span, arbor_stream stream);
+
+/* Leaf nodes 32768+i from Morton order (Arbor.cu:141; bindings P r, Order r,
+ * Nodes w). */
+ARBOR_API int arbor_makeBounds(const float* P, const uint32_t* Order, float* Nodes, arbor_stream stream);
+
+/* One BVH level: parents first..2*first-1 (Arbor.cu:142; bindings Nodes rw;
+ * scalar first).  first must lie in 0..16384. */
+ARBOR_API int arbor_reduceBounds(float* Nodes, int first, arbor_stream stream);
+
+/* Camera/state record defaults (Arbor.cu:181; bindings C w, P r; scalar seed). */
+ARBOR_API int arbor_initCamera(float* C, const float* P, int seed, arbor_stream stream);
+
+/* Input record -> camera state (Arbor.cu:182; bindings C rw, I r, P r;
+ * scalars delta (finite), width, height). */
+ARBOR_API int arbor_updateCamera(float* C, const float* I, const float* P, float delta, int width, int height, arbor_stream stream);
+
+/* Primary hit per pixel: Hit[4*px] = {t, primId, treeId, footprint}
+ * (Arbor.cu:252; bindings P, Nodes, Order, C r; Hit w; scalars width, height). */
+ARBOR_API int arbor_tracePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height, arbor_stream stream);
+
+/* Radiance and albedo per pixel, sun shadows when C[22] > 0.5
+ * (Arbor.cu:277-289; bindings P, Nodes, Order, C, Hit r; Linear, Guide w). */
+ARBOR_API int arbor_shadePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, arbor_stream stream);
+
+/* 5x5 same-surface demodulated filter (Arbor.cu:292-302; bindings Linear,
+ * Guide, Hit r; Filtered w; C r). */
+ARBOR_API int arbor_filterLighting(const float* Linear, const float* Guide, const float* Hit, float* Filtered, const float* C, int width, int height, arbor_stream stream);
+
+/* Progressive mean, ACES, gamma, vignette, RGBA8 (Arbor.cu:303-304; bindings
+ * Filtered r, History rw, Pixels w, C r). */
+ARBOR_API int arbor_resolvePixels(const float* Filtered, float* History, uint32_t* Pixels, const float* C, int width, int height, arbor_stream stream);
+
+/* ---------------------------------------------------------------------------
+ * Fused and extra entry points (no single reference counterpart).
+ * ------------------------------------------------------------------------- */
+
+/* Stable LSD radix sort of (Keys, Order) by key: the same (key, index) order
+ * as the reference's 120 bitonic sortPass stages (src/engine.js:31) and the
+ * harness's std::sort of pairs (tests/native_harness.cpp:47), provided Order
+ * holds increasing indices on entry, as makeKeys leaves it.  `scratch` is
+ * caller-owned device memory of at least arbor_sort_scratch_bytes() bytes. */
+ARBOR_API size_t arbor_sort_scratch_bytes(void);
+ARBOR_API int arbor_sortKeys(uint32_t* Keys, uint32_t* Order, void* scratch, arbor_stream stream);
+
+/* Makes leaf nodes (as makeBounds) and all 15 parent levels (as the 15
+ * reduceBounds dispatches, src/engine.js:32) in two launches. */
+ARBOR_API int arbor_buildBounds(const float* P, const uint32_t* Order, float* Nodes, arbor_stream stream);
+
+/* The whole scene build of src/engine.js:27-33 for one seed: growTree x5,
+ * makePrimitives, makeKeys, sort, makeBounds, reduceBounds x15, initCamera.
+ * Bit-identical Keys/Order/Nodes to the reference sequence given the same P.
+ * B must be zeroed by the caller before the first build (the reference's
+ * buffers start zeroed); `scratch` as for arbor_sortKeys.  C may be NULL to
+ * leave the camera untouched. */
+ARBOR_API int arbor_buildScene(int seed, float* B, float* P, uint32_t* Keys, uint32_t* Order, float* Nodes, float* C, void* scratch, arbor_stream stream);
+
+/* Single-tree scene (no reference counterpart; mirrors the harness's direct
+ * traceTree use at tests/native_harness.cpp:84): the resident tree traced
+ * with an identity instance.  Hit.treeId is -1; shading uses the tree-local
+ * normal, no per-tree tint, and shadow rays through the same tree. */
+ARBOR_API int arbor_traceTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height, arbor_stream stream);
+ARBOR_API int arbor_shadeTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, arbor_stream stream);
+
+/* filterLighting followed by resolvePixels in one launch; writes Filtered,
+ * History and Pixels exactly as the two separate entries do. */
+ARBOR_API int arbor_filterResolve(const float* Linear, const float* Guide, const float* Hit, float* Filtered, float* History, uint32_t* Pixels, const float* C, int width, int height, arbor_stream stream);
+
+/* ---------------------------------------------------------------------------
+ * Engine: the C++ host of src/engine.js (generate / resize / frame /
+ * inspect / dispose) over the entries above.
+ * ------------------------------------------------------------------------- */
+typedef struct arbor_engine arbor_engine;
+
+typedef struct arbor_engine_buffers {
+  float* B; float* P; uint32_t* Keys; uint32_t* Order; float* Nodes; float* C; float* I;
+  float* Hit; float* Linear; float* Guide; float* Filtered; float* History; uint32_t* Pixels;
+} arbor_engine_buffers;
+
+typedef struct arbor_engine_info {
+  int width, height, seed, single_tree;
+  uint64_t frames;
+  uint64_t allocated_bytes;     /* all engine device buffers */
+  uint64_t scene_bytes;         /* B + P + Keys + Order + Nodes (src/engine.js:55) */
+  uint32_t launches_per_frame;  /* kernels one arbor_engine_frame launches */
+  float camera[64];             /* copy of C after the last frame */
+  float ms_build, ms_visibility, ms_lighting, ms_resolve; /* last timed phases */
+} arbor_engine_info;
+
+/* Creates an engine on the current device: allocates the ABI buffers for
+ * width x height (rounded as src/engine.js:36: width up to a multiple of 64,
+ * at least 320; height up to a multiple of 8, at least 192) and builds the
+ * scene for `seed` (integer 0..1,000,000, src/engine.js:28).  single_tree != 0
+ * selects the one-tree scene. */
+ARBOR_API int arbor_engine_create(arbor_engine** out, int width, int height, int seed, int single_tree, arbor_stream stream);
+ARBOR_API int arbor_engine_generate(arbor_engine* e, int seed);
+ARBOR_API int arbor_engine_resize(arbor_engine* e, int width, int height);
+/* Copies a 32-float input record (host memory) into I for the next frame. */
+ARBOR_API int arbor_engine_set_input(arbor_engine* e, const float* input32);
+/* Overwrites the 64-float camera/state record C from host memory, as the
+ * harness writes Renderer::c directly (tests/native_harness.cpp:61-62). */
+ARBOR_API int arbor_engine_set_state(arbor_engine* e, const float* state64);
+/* One frame: updateCamera, trace, shade, filter+resolve (src/engine.js:45-53). */
+ARBOR_API int arbor_engine_frame(arbor_engine* e, float dt);
+/* Per-phase CUDA-event timing of subsequent frames on/off. */
+ARBOR_API int arbor_engine_set_timing(arbor_engine* e, int enabled);
+ARBOR_API int arbor_engine_inspect(arbor_engine* e, arbor_engine_info* info);
+ARBOR_API int arbor_engine_buffers_get(arbor_engine* e, arbor_engine_buffers* out);
+/* Copies Pixels to host memory (width*height uint32) on the engine stream
+ * and waits for it. */
+ARBOR_API int arbor_engine_read_pixels(arbor_engine* e, uint32_t* host, size_t count);
+/* Releases the engine's device memory (src/engine.js:57); the handle stays
+ * valid and every later call on it returns ARBOR_ERR_STATE. */
+ARBOR_API int arbor_engine_dispose(arbor_engine* e);
+/* Disposes (if needed) and frees the handle. */
+ARBOR_API int arbor_engine_destroy(arbor_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ARBOR_H */

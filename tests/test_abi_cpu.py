@@ -1,0 +1,113 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol the header
+declares, and rejects bad arguments before touching the device (the checks
+of vendor/cuda-webshader/runtime/runtime.js:18-22, 323-325, 352).
+
+Every call here fails validation, so no kernel is launched; the fake device
+addresses are never dereferenced.
+"""
+import ctypes
+import os
+import re
+
+import pytest
+
+import arbor_b200 as ab
+
+HEADER = os.path.join(os.path.dirname(__file__), "..", "include", "arbor.h")
+A = 0x10000000  # fake, 256-byte aligned device addresses (never dereferenced)
+MB = 1 << 20
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(arbor_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return ab.lib()
+
+
+def test_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len(names) >= 12 + 10
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(ab.SIGNATURES), set(names) ^ set(ab.SIGNATURES)
+
+
+def test_the_twelve_reference_entries_are_declared():
+    names = declared_functions()
+    for entry in ("growTree", "makePrimitives", "makeKeys", "sortPass", "makeBounds", "reduceBounds", "initCamera",
+                  "updateCamera", "tracePixels", "shadePixels", "filterLighting", "resolvePixels"):
+        assert f"arbor_{entry}" in names
+
+
+def test_status_names(lib):
+    assert lib.arbor_status_name(0) == b"ARBOR_OK"
+    assert lib.arbor_status_name(4) == b"ARBOR_ERR_ALIAS"
+    assert lib.arbor_status_name(99) == b"ARBOR_ERR_UNKNOWN"
+    assert lib.arbor_sort_scratch_bytes() == 2 * 32768 * 4
+
+
+def test_null_buffers_rejected(lib):
+    assert lib.arbor_tracePixels(None, A, A + 4 * MB, A + 8 * MB, A + 16 * MB, 64, 64, None) == ab.ERR_NULL
+    assert b"P" in lib.arbor_last_error()
+    assert lib.arbor_growTree(None, 0, 1, None) == ab.ERR_NULL
+    assert lib.arbor_makeKeys(A, None, A + 8 * MB, None) == ab.ERR_NULL
+
+
+def test_misaligned_buffers_rejected(lib):
+    assert lib.arbor_tracePixels(A + 4, A + 4 * MB, A + 8 * MB, A + 9 * MB, A + 16 * MB, 64, 64, None) == ab.ERR_ALIGN
+    assert lib.arbor_makePrimitives(A + 2, A + 4 * MB, 1, None) == ab.ERR_ALIGN
+
+
+def test_writable_aliasing_rejected(lib):
+    # Hit overlapping P (runtime.js:325)
+    assert lib.arbor_tracePixels(A, A + 4 * MB, A + 8 * MB, A + 9 * MB, A + 64, 64, 64, None) == ab.ERR_ALIAS
+    assert b"aliasing" in lib.arbor_last_error()
+    # Keys and Order the same buffer
+    assert lib.arbor_sortPass(A, A, 1, 2, None) == ab.ERR_ALIAS
+    # filter writing into its own input
+    assert lib.arbor_filterLighting(A, A + 4 * MB, A + 8 * MB, A, A + 12 * MB, 64, 64, None) == ab.ERR_ALIAS
+
+
+def test_read_only_aliasing_allowed_until_launch(lib):
+    """Two read-only bindings may share a buffer (runtime.js:325 rejects only
+    writable aliasing): with width 0 the call validates and returns without a
+    launch."""
+    assert lib.arbor_tracePixels(A, A, A + 8 * MB, A + 9 * MB, A + 16 * MB, 0, 64, None) == ab.OK
+
+
+def test_scalar_ranges(lib):
+    assert lib.arbor_sortPass(A, A + MB, 32768, 2, None) == ab.ERR_VALUE
+    assert lib.arbor_sortPass(A, A + MB, -1, 2, None) == ab.ERR_VALUE
+    assert lib.arbor_reduceBounds(A, 16385, None) == ab.ERR_VALUE
+    assert lib.arbor_reduceBounds(A, -1, None) == ab.ERR_VALUE
+    assert lib.arbor_reduceBounds(A, 0, None) == ab.OK  # nothing to reduce: no launch
+    assert lib.arbor_updateCamera(A, A + MB, A + 2 * MB, float("nan"), 64, 64, None) == ab.ERR_VALUE
+    assert lib.arbor_updateCamera(A, A + MB, A + 2 * MB, float("inf"), 64, 64, None) == ab.ERR_VALUE
+
+
+def test_image_sizes(lib):
+    args = (A, A + 4 * MB, A + 8 * MB, A + 9 * MB, A + 16 * MB)
+    assert lib.arbor_tracePixels(*args, -1, 64, None) == ab.ERR_VALUE
+    assert lib.arbor_tracePixels(*args, 64, 0, None) == ab.OK  # zero workgroups: no-op
+    assert lib.arbor_tracePixels(*args, 65536 * 8 + 1, 8, None) == ab.ERR_LIMIT  # > 65535 workgroups
+    assert lib.arbor_resolvePixels(A, A + 4 * MB, A + 8 * MB, A + 9 * MB, 30000, 30000, None) == ab.ERR_LIMIT
+
+
+def test_engine_rejections_without_device(lib):
+    h = ctypes.c_void_p()
+    st = lib.arbor_engine_create(ctypes.byref(h), 640, 360, 1, 0, None)
+    if lib.arbor_device_ready():
+        pytest.skip("a device is present; covered by the GPU engine tests")
+    assert st == ab.ERR_NO_DEVICE and not h.value
+    assert lib.arbor_engine_create(None, 640, 360, 1, 0, None) == ab.ERR_NULL
+    assert lib.arbor_engine_frame(None, 0.016) == ab.ERR_NULL
+    assert lib.arbor_engine_destroy(None) == ab.OK
+
+
+def test_launch_counter_starts_without_launches(lib):
+    assert lib.arbor_launch_count() >= 0

@@ -1,0 +1,160 @@
+"""Scene build on the GPU against the CPU oracle (pinned to the reference).
+
+Contract (the reference's own definition of "same scene"):
+  - makeKeys, the sort, makeBounds and reduceBounds are bit-exact given the
+    same P (they use only + - * / min max);
+  - growTree/makePrimitives use sin/cos/pow; the GPU's are correctly rounded
+    and glibc's are not always, so B and P agree within 2 ulp on a few percent
+    of floats, and the Morton keys, order and BVH topology built from the
+    GPU's own P are still bit-exact (checked on every seed below).
+"""
+import numpy as np
+import pytest
+
+from conftest import u32
+
+pytestmark = pytest.mark.gpu
+
+SEEDS = [1, 7, 1788, 42]
+
+
+@pytest.fixture(scope="module")
+def gu():
+    import gpu_util
+
+    return gpu_util
+
+
+def test_grow_levels_from_oracle_parents(cuda, oracle, scenes, gu):
+    s = scenes(1788)
+    B_ref = np.zeros(2109 * 20, np.float32)
+    for level in range(5):
+        before = B_ref.copy()
+        oracle.grow(B_ref, level, 1788)
+        B = gu.dev(before)
+        gu.ok(cuda.call("arbor_growTree", B, level, 1788))
+        got = gu.host(B)
+        d = gu.ulp_diff(got, B_ref)
+        assert d.max() <= 2, f"level {level}: max ulp {d.max()}"
+        assert np.mean(d > 0) < 0.05
+    assert np.array_equal(B_ref, s["B"])
+
+
+def test_primitives_wood_exact_leaves_close(cuda, oracle, scenes, gu):
+    s = scenes(7)
+    P = gu.zeros_f(32768 * 24)
+    gu.ok(cuda.call("arbor_makePrimitives", gu.dev(s["B"]), P, 7))
+    got = gu.host(P).reshape(32768, 24)
+    want = s["P"].reshape(32768, 24)
+    # wood records use no transcendental function: bit-exact
+    assert np.array_equal(u32(got[:5124]), u32(want[:5124]))
+    assert np.array_equal(u32(got[29412:]), u32(want[29412:]))
+    d = gu.ulp_diff(got, want)
+    assert d.max() <= 2 and np.mean(d > 0) < 0.05
+    assert np.array_equal(got[:, 3], want[:, 3])
+
+
+@pytest.mark.parametrize("seed", SEEDS)
+def test_keys_exact_given_P(cuda, scenes, gu, seed):
+    s = scenes(seed)
+    keys, order = gu.zeros_u(32768), gu.zeros_u(32768)
+    gu.ok(cuda.call("arbor_makeKeys", gu.dev(s["P"]), keys, order))
+    assert np.array_equal(gu.host(keys, np.uint32), s["RawKeys"])
+    assert np.array_equal(gu.host(order, np.uint32), np.arange(32768, dtype=np.uint32))
+
+
+def test_bitonic_stages_exact(cuda, scenes, gu):
+    s = scenes(1)
+    keys, order = gu.dev(s["RawKeys"]), gu.dev(np.arange(32768, dtype=np.uint32))
+    stages = 0
+    span = 2
+    while span <= 32768:
+        d = span // 2
+        while d > 0:
+            gu.ok(cuda.call("arbor_sortPass", keys, order, d, span))
+            stages += 1
+            d //= 2
+        span *= 2
+    assert stages == 120
+    assert np.array_equal(gu.host(keys, np.uint32), s["Keys"])
+    assert np.array_equal(gu.host(order, np.uint32), s["Order"])
+
+
+@pytest.mark.parametrize("seed", SEEDS)
+def test_radix_sort_equals_bitonic_order(cuda, scenes, gu, seed):
+    s = scenes(seed)
+    keys, order = gu.dev(s["RawKeys"]), gu.dev(np.arange(32768, dtype=np.uint32))
+    scratch = gu.zeros_u(2 * 32768)
+    gu.ok(cuda.call("arbor_sortKeys", keys, order, scratch))
+    assert np.array_equal(gu.host(keys, np.uint32), s["Keys"])
+    assert np.array_equal(gu.host(order, np.uint32), s["Order"])
+
+
+def test_radix_sort_edge_keys(cuda, oracle, gu):
+    """All-equal keys (pure tie-break by index), all-unused keys, and keys
+    spanning every byte."""
+    rng = np.random.default_rng(5)
+    cases = [np.zeros(32768, np.uint32), np.full(32768, 0xFFFFFFFF, np.uint32),
+             rng.integers(0, 2**32, 32768, dtype=np.uint64).astype(np.uint32),
+             rng.integers(0, 4, 32768).astype(np.uint32) << np.uint32(24)]
+    for raw in cases:
+        k_ref, o_ref = raw.copy(), np.arange(32768, dtype=np.uint32)
+        oracle.sort_pairs(k_ref, o_ref)
+        keys, order = gu.dev(raw), gu.dev(np.arange(32768, dtype=np.uint32))
+        gu.ok(cuda.call("arbor_sortKeys", keys, order, gu.zeros_u(2 * 32768)))
+        assert np.array_equal(gu.host(keys, np.uint32), k_ref)
+        assert np.array_equal(gu.host(order, np.uint32), o_ref)
+
+
+@pytest.mark.parametrize("seed", [1, 1788])
+def test_bounds_levels_exact(cuda, scenes, gu, seed):
+    s = scenes(seed)
+    nodes = gu.zeros_f(65536 * 8)
+    P, order = gu.dev(s["P"]), gu.dev(s["Order"])
+    gu.ok(cuda.call("arbor_makeBounds", P, order, nodes))
+    first = 16384
+    while first >= 1:
+        gu.ok(cuda.call("arbor_reduceBounds", nodes, first))
+        first //= 2
+    assert np.array_equal(u32(gu.host(nodes)), u32(s["Nodes"]))
+    nodes2 = gu.zeros_f(65536 * 8)
+    gu.ok(cuda.call("arbor_buildBounds", P, order, nodes2))
+    assert np.array_equal(u32(gu.host(nodes2)), u32(s["Nodes"]))
+
+
+@pytest.mark.parametrize("seed", SEEDS + [0, 999999])
+def test_build_scene_end_to_end(cuda, oracle, gu, seed):
+    s = oracle.build_scene(seed)
+    d = gu.DevScene()
+    C = gu.zeros_f(64)
+    gu.ok(cuda.call("arbor_buildScene", seed, d.B, d.P, d.Keys, d.Order, d.Nodes, C, gu.zeros_u(2 * 32768)))
+    keys, order = gu.host(d.Keys, np.uint32), gu.host(d.Order, np.uint32)
+    assert np.array_equal(keys, s["Keys"]), f"seed {seed}: {np.count_nonzero(keys != s['Keys'])} keys differ"
+    assert np.array_equal(order, s["Order"])
+    nodes = gu.host(d.Nodes).reshape(-1, 8)
+    want = s["Nodes"].reshape(-1, 8)
+    assert np.array_equal(nodes[1:, 3], want[1:, 3]), "BVH counts"
+    assert np.array_equal(nodes[1:, 7], want[1:, 7]), "leaf ids / internal markers"
+    assert gu.ulp_diff(nodes[1:, [0, 1, 2, 4, 5, 6]], want[1:, [0, 1, 2, 4, 5, 6]]).max() <= 4
+    P = gu.host(d.P)
+    assert gu.ulp_diff(P, s["P"]).max() <= 2
+    Cw = oracle.init_camera(s["P"], seed)
+    assert np.array_equal(u32(gu.host(C)), u32(Cw))
+
+
+def test_grow_any_level_matches_kernel_semantics(cuda, oracle, scenes, gu):
+    """Levels outside 0..4 act as level 4 with the kernel's own constants."""
+    s = scenes(1)
+    for level in (5, -3):
+        B_ref = s["B"].copy()
+        oracle.grow(B_ref, level, 1)
+        B = gu.dev(s["B"])
+        gu.ok(cuda.call("arbor_growTree", B, level, 1))
+        assert gu.ulp_diff(gu.host(B), B_ref).max() <= 2
+
+
+def test_sortpass_distance_zero_is_identity(cuda, scenes, gu):
+    raw = scenes(1)["RawKeys"]
+    keys, order = gu.dev(raw), gu.dev(np.arange(32768, dtype=np.uint32))
+    gu.ok(cuda.call("arbor_sortPass", keys, order, 0, 2))
+    assert np.array_equal(gu.host(keys, np.uint32), raw)

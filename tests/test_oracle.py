@@ -1,0 +1,211 @@
+"""CPU oracle pinned to the reference (no GPU).
+
+The oracle port (oracle/arbor_oracle.c) must reproduce the golden digests
+made from the reference's own harness code (tests/golden/make_golden.py),
+and, where the reference build is available here, match it buffer for
+buffer.  The harness's own checks (tests/native_harness.cpp:65-95, minus
+the stale orbit-camera check at :72-73) are restated against the oracle.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import u32
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_golden.json")))
+CAP, PS = 32768, 24
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("seed", [0, 1, 7, 42, 1788])
+def test_scene_matches_golden(oracle, scenes, seed):
+    s = scenes(seed)
+    g = GOLD["scenes"][str(seed)]
+    for k in ("B", "P", "Keys", "Order", "Nodes", "RawKeys"):
+        assert digest(s[k]) == g[k], f"seed {seed} buffer {k} differs from the reference"
+
+
+def test_recorded_bounds_seed_1788(scenes):
+    # docs/native-checks.log:2  BOUNDS -5.50279,-0.832,-5.30197 to 5.40578,11.2203,5.22893
+    n = scenes(1788)["Nodes"]
+    np.testing.assert_allclose(n[8:11], [-5.50279, -0.832, -5.30197], atol=5e-6)
+    np.testing.assert_allclose(n[12:15], [5.40578, 11.2203, 5.22893], atol=5e-5)
+
+
+@pytest.mark.parametrize("name", sorted(GOLD["frames_1788_96x64"]))
+def test_forest_frames_match_golden(oracle, scenes, name):
+    g = GOLD["frames_1788_96x64"][name]
+    C = np.array(g["C"], np.float32)
+    f = oracle.frame(scenes(1788), C, 96, 64)
+    for k in ("Hit", "Linear", "Guide", "Filtered", "History", "Pixels"):
+        assert digest(f[k]) == g[k], f"{name}: {k} differs from the reference"
+
+
+@pytest.mark.parametrize("key", ["tree_seed1_128", "tree_seed1_128_shadows"])
+def test_single_tree_frame_matches_golden(oracle, scenes, key):
+    g = GOLD[key]
+    C = np.array(g["C"], np.float32)
+    f = oracle.frame(scenes(1), C, 128, 128, single=True)
+    for k in ("Hit", "Linear", "Guide", "Filtered", "History", "Pixels"):
+        assert digest(f[k]) == g[k], f"{key}: {k} differs"
+
+
+def test_camera_walk_matches_golden(oracle, scenes):
+    import workloads
+
+    P = scenes(7)["P"]
+    C = oracle.init_camera(P, 7)
+    for frame, want in enumerate(GOLD["walk_seed7_C"]):
+        I, dt = workloads.walk_input(frame)
+        oracle.update_camera(C, I, P, dt, 192, 108)
+        assert np.array_equal(u32(C), u32(np.array(want, np.float32))), f"frame {frame}"
+
+
+def test_instances_and_tree_seeds(oracle):
+    assert [oracle.forest_seed(t, 7) for t in range(324)] == GOLD["forest_seeds_seed7"]
+    for t, want in zip((0, 1, 17, 100, 161, 162, 323), GOLD["instances_seed7"]):
+        assert np.array_equal(u32(oracle.forest_instance(t, 7)), u32(np.array(want, np.float32)))
+
+
+# ---- harness checks (tests/native_harness.cpp:65-95) against the oracle ----
+def test_primitives_finite_and_counts(scenes):
+    P = scenes(1788)["P"]
+    assert np.isfinite(P).all()
+    types = P.reshape(CAP, PS)[:, 3]
+    assert (types == 0).sum() == 5124 and (types == 1).sum() == 24192 and (types == 2).sum() == 96
+    assert (types == -1).sum() == CAP - 29412
+
+
+def test_root_count_and_containment(scenes):
+    n = scenes(1788)["Nodes"].reshape(-1, 8)
+    assert n[1, 3] == 29412
+    parent = np.arange(1, CAP)
+    for c in (0, 1):
+        child = n[parent * 2 + c]
+        act = child[:, 3] > 0
+        assert (child[act, 0:3] >= n[parent[act], 0:3] - 1e-5).all()
+        assert (child[act, 4:7] <= n[parent[act], 4:7] + 1e-5).all()
+
+
+def test_camera_presets_leave_geometry(oracle, scenes):
+    s = scenes(1788)
+    P0 = s["P"].copy()
+    C = oracle.init_camera(s["P"], 1788)
+    for view in range(1, 6):
+        I = np.zeros(32, np.float32)
+        I[5] = view
+        oracle.update_camera(C, I, s["P"], 1 / 60, 960, 720)
+    assert np.array_equal(P0, s["P"])
+
+
+def test_other_seed_changes_layout(scenes):
+    a, b = scenes(1788), scenes(42)
+    assert not np.array_equal(a["P"], b["P"])
+    assert b["Nodes"][11] == 29412
+
+
+def test_bitonic_equals_independent_sort(oracle, scenes):
+    s = scenes(1)
+    k, o = s["RawKeys"].copy(), np.arange(CAP, dtype=np.uint32)
+    oracle.bitonic(k, o)
+    assert np.array_equal(k, s["Keys"]) and np.array_equal(o, s["Order"])
+    raw = s["RawKeys"]
+    assert len(raw[raw != 0xFFFFFFFF]) - len(np.unique(raw[raw != 0xFFFFFFFF])) == 763
+
+
+def test_bvh_rays_match_exhaustive(oracle, scenes):
+    s = scenes(1788)
+    worst = 0.0
+    for r in GOLD["harness_rays_1788"]:
+        ro, rd = np.array(r["ro"], np.float32), np.array(r["rd"], np.float32)
+        t, oid = oracle.trace_tree_ray(s, ro, rd, 0.0005)
+        et, eid = oracle.exhaustive_ray(s["P"], ro, rd, 0.0005)
+        assert (oid < 0) == (eid < 0) and abs(et - t) <= 0.002
+        assert (t, oid) == (r["t"], r["id"])
+        if t < 1e5 and et < 1e5:
+            worst = max(worst, abs(et - t))
+    assert worst == GOLD["harness_bvh_max_t_error"] == 0.0
+
+
+def test_harness_rays_reproduced(oracle):
+    for i, r in enumerate(GOLD["harness_rays_1788"]):
+        ro, rd = oracle.harness_ray(i)
+        assert ro.tolist() == r["ro"] and rd.tolist() == r["rd"]
+
+
+def test_footprint_sweep(oracle, scenes):
+    jump, mono, finite = oracle.footprint_sweep(scenes(1788)["P"], 4)
+    assert mono and finite and jump < 5e-5
+    assert jump == pytest.approx(GOLD["footprint_sweep"]["max_jump"], abs=0)
+    assert abs(jump - 7.73836e-06) < 5e-11  # docs/native-checks.log:14
+
+
+def test_leaves_near_and_far(oracle, scenes):
+    P = scenes(1788)["P"]
+    for k, want in enumerate(GOLD["leaf_pairs"]):
+        a, c = oracle.leaf_pair(P, k)
+        assert a < 1e5 and c < 1e5 and abs(a - c) < 0.002
+        assert [a, c] == want
+
+
+def test_hdr_frame_finite_nonnegative(oracle, scenes):
+    s = scenes(1788)
+    C = oracle.init_camera(s["P"], 1788)
+    I = np.zeros(32, np.float32)
+    I[5] = 1
+    oracle.update_camera(C, I, s["P"], 1 / 60, 160, 120)
+    f = oracle.frame(s, C, 160, 120)
+    assert np.isfinite(f["Linear"]).all() and (f["Linear"] >= 0).all()
+    px = f["Pixels"]
+    assert ((px >> 24) == 255).all()
+
+
+# ---- oracle port == reference build, where the reference is present ----
+@pytest.mark.parametrize("seed", [3, 1000000])
+def test_port_equals_reference_build(oracle, ref, seed):
+    a, b = oracle.build_scene(seed), ref.build_scene(seed)
+    for k in ("B", "P", "Keys", "Order", "Nodes"):
+        assert np.array_equal(u32(a[k]), u32(b[k])), k
+
+
+def test_port_equals_reference_walk_frames(oracle, ref, scenes):
+    import workloads
+
+    s = scenes(7)
+    Ca = oracle.init_camera(s["P"], 7)
+    Cb = ref.init_camera(s["P"], 7)
+    for frame in range(3):
+        I, dt = workloads.walk_input(frame)
+        oracle.update_camera(Ca, I, s["P"], dt, 120, 68)
+        ref.update_camera(Cb, I, s["P"], dt, 120, 68)
+        assert np.array_equal(u32(Ca), u32(Cb))
+    Ca[22] = 1.0
+    fa = oracle.frame(s, Ca, 120, 68)
+    fb = ref.frame(s, Ca.copy(), 120, 68)
+    for k in fa:
+        assert np.array_equal(u32(fa[k]), u32(fb[k])), k
+
+
+def test_f64_rerun_close_to_f32(oracle, oracle64, scenes):
+    """The FP64 instantiation runs the same formulas in double.
+
+    The leaf Newton solve and the SDF march accept or reject a hit by
+    thresholds on float residuals, so working precision alone moves a few
+    percent of hit IDs (measured: 96.9% agreement at 96x64, view 2); on the
+    pixels whose IDs agree, hit distances agree closely.
+    """
+    s = scenes(1788)
+    C = np.array(GOLD["frames_1788_96x64"]["view2_light0_mode0"]["C"], np.float32)
+    h32 = oracle.trace(s, C, 96, 64).reshape(-1, 4)
+    h64 = oracle64.trace(s, C, 96, 64).reshape(-1, 4)
+    same = (h32[:, 1] == h64[:, 1]) & (h32[:, 2] == h64[:, 2])
+    assert same.mean() > 0.95
+    both = same & (h32[:, 0] < 1e5)
+    rel = np.abs(h32[both, 0] - h64[both, 0]) / h64[both, 0]
+    assert np.median(rel) < 1e-5 and np.quantile(rel, 0.99) < 2e-3
