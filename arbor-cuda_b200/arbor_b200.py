@@ -69,6 +69,8 @@ SIGNATURES = {
     "arbor_traceTreePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_shadeTreePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_filterResolve": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
+    "arbor_trace_work_slots": (ctypes.c_size_t, [_i, _i]),
+    "arbor_traceWork": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
     "arbor_engine_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, _vp]),
     "arbor_engine_generate": (_i, [_vp, _i]),
     "arbor_engine_resize": (_i, [_vp, _i, _i]),

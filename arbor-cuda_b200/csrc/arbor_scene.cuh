@@ -8,7 +8,30 @@
 #pragma once
 #include "arbor_math.cuh"
 
+// Work-event hooks.  They compile to nothing in the product kernels; the
+// work-counting translation unit (count.cu) defines ARBOR_COUNT before
+// including this header to tally the events the trace roofline model weighs.
+#ifndef ARBOR_COUNT
+#define ARBOR_COUNT(event) ((void)0)
+#endif
+
 namespace arbor {
+
+enum WorkEvent {
+  kEvRay = 0,          // primary ray set up
+  kEvCell = 1,         // forest DDA cell with its bounding-sphere test
+  kEvTree = 2,         // tree entered (local transform + root test)
+  kEvNode = 3,         // BVH node box test
+  kEvWood = 4,         // primary wood test (frame, tube, bounds)
+  kEvMarch = 5,        // SDF march step (one woodField)
+  kEvBarkFull = 6,     // bark relief past its footprint early-out
+  kEvWoodShadow = 7,   // shadow-ray wood tube test
+  kEvLeaf = 8,         // leaf test (frame, petiole tube, box clip)
+  kEvNewtonStart = 9,  // leaf test that reaches the Newton solve
+  kEvNewton = 10,      // Newton iteration (five height-field evaluations)
+  kEvStone = 11,       // stone ellipsoid test
+  kEvCount = 12
+};
 
 // ------------------------------------------------------------ records --
 __device__ __forceinline__ float4 ldg4(const float* base, int index4) {
@@ -83,6 +106,7 @@ __device__ __forceinline__ float bark_cut(const Wood& w, f3 p, float fp, float f
   float period = radius * 2.0f * kPi / (float)w.columns;
   float coarse = band_weight(period, fp);
   if (coarse < 0.000001f && fine < 0.000001f) return amp * 0.32f;
+  ARBOR_COUNT(kEvBarkFull);
   float z = dot3(pa, w.d);
   float theta = atan2f(dot3(pa, w.v), dot3(pa, w.u));
   float arc = w.arc0 + z;
@@ -220,12 +244,14 @@ __device__ __forceinline__ float tube_t(f3 ro, f3 rd, f3 a, f3 b, float ra, floa
 // SDF march seeded by the analytic tube for primary rays.
 static __device__ __noinline__ float wood_t(const float* P, int id, f3 ro, f3 rd, float footprint, bool refine) {
   if (!refine) {
+    ARBOR_COUNT(kEvWoodShadow);
     float4 r0 = ldg4(P, id * 6 + 0), r1 = ldg4(P, id * 6 + 1), r2 = ldg4(P, id * 6 + 2);
     float p7 = r1.w, p11 = r2.w;
     float ra = p7 - fminf(0.021f, p7 * 0.055f) * 0.32f;
     float rb = p11 - fminf(0.021f, p11 * 0.055f) * 0.32f;
     return tube_t(ro, rd, xyz(r0), xyz(r1), ra, rb);
   }
+  ARBOR_COUNT(kEvWood);
   Wood w = load_wood(P, id);
   float t = tube_t(ro, rd, w.a, w.end, w.ra, w.rb);
   if (t >= kFar) return kFar;
@@ -240,6 +266,7 @@ static __device__ __noinline__ float wood_t(const float* P, int id, f3 ro, f3 rd
   float fine = band_weight(0.010f, footprint);
   float grain = band_weight(0.0025f, footprint);
   for (int k = 0; k < 64; k++) {
+    ARBOR_COUNT(kEvMarch);
     float f = wood_field(w, ro + rd * t, footprint, fine, grain);
     if (f < eps) return t;
     t += fmaxf(eps * 0.35f, f * 0.27f);
@@ -249,6 +276,7 @@ static __device__ __noinline__ float wood_t(const float* P, int id, f3 ro, f3 rd
 }
 // Curved-leaf Newton solve (Arbor.cu:203-218).
 static __device__ __noinline__ float leaf_t(const float* P, int id, f3 ro, f3 rd, float footprint, float time, float wind) {
+  ARBOR_COUNT(kEvLeaf);
   Leaf l = load_leaf(P, id, time, wind);
   f3 q = ro - l.origin;
   float x = dot3(q, l.u) - l.stem;
@@ -260,11 +288,13 @@ static __device__ __noinline__ float leaf_t(const float* P, int id, f3 ro, f3 rd
   float best = tube_t(ro, rd, l.origin, l.origin + l.u * l.stem, 0.0011f, 0.00065f);
   f2 span = box_span(mk(x, y, z), mk(dx, dy, dz), mk(-0.001f, -l.width, -0.035f), mk(l.len + 0.001f, l.width, 0.065f));
   if (span.y < fmaxf(0.0001f, span.x)) return best;
+  ARBOR_COUNT(kEvNewtonStart);
   float t = fabsf(dz) > 0.000001f ? -z / dz : (span.x + span.y) * 0.5f;
   t = clampf(t, fmaxf(0.0001f, span.x), span.y);
   float hw2 = l.width * l.width;
   float bw007 = band_weight(0.007f, footprint);
   for (int k = 0; k < 7; k++) {
+    ARBOR_COUNT(kEvNewton);
     float xx = x + dx * t;
     float yy = y + dy * t;
     float height = leaf_height(xx, yy, l.len, hw2, l.curl, l.twist, bw007);
@@ -291,6 +321,7 @@ __device__ __forceinline__ float object_t(const float* P, int id, f3 ro, f3 rd, 
   if (type < 0) return kFar;
   if (type == 0) return wood_t(P, id, ro, rd, footprint, refine);
   if (type == 1) return leaf_t(P, id, ro, rd, footprint, time, wind);
+  ARBOR_COUNT(kEvStone);
   f3 h = xyz(ldg4(P, id * 6 + 1));
   f3 q = ro - xyz(r0);
   f3 p = mk(q.x / h.x, q.y / h.y, q.z / h.z);
@@ -320,6 +351,7 @@ __device__ __forceinline__ float object_t(const float* P, int id, f3 ro, f3 rd, 
 // repeats the child test just made with the same best, so it always passes;
 // its span.x (the leaf footprint input) is carried instead.
 __device__ __forceinline__ bool node_accept(float4 lo, float4 hi, f3 ro, f3 inv, float best, float& spanx) {
+  ARBOR_COUNT(kEvNode);
   f2 s = box_span_inv(ro, inv, xyz(lo), xyz(hi));
   spanx = s.x;
   return lo.w > 0.0f && s.y >= fmaxf(0.0001f, s.x) && s.x < best;
@@ -420,9 +452,11 @@ __device__ __forceinline__ f2 trace_forest(const float* P, const float* Nodes, c
   for (int step = 0; step < 48; step++) {
     if (ix < 0 || iz < 0 || ix >= kSide || iz >= kSide) break;
     int tree = iz * kSide + ix;
+    ARBOR_COUNT(kEvCell);
     const Instance& it = inst[tree];
     float broad = sphere_t(ro, rd, mk(it.px + 0.0f, 0.0f + it.cy, it.pz + 0.0f), it.rad);
     if (broad < best) {
+      ARBOR_COUNT(kEvTree);
       f3 lr = to_local_point(ro, it);
       f3 ld = to_local_dir(rd, it);
       f2 h = trace_tree(P, Nodes, Order, lr, ld, cone / it.sc, time + it.phase, wind, best / it.sc, -1, shadows);

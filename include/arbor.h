@@ -178,6 +178,16 @@ ARBOR_API int arbor_shadeTreePixels(const float* P, const float* Nodes, const ui
  * History and Pixels exactly as the two separate entries do. */
 ARBOR_API int arbor_filterResolve(const float* Linear, const float* Guide, const float* Hit, float* Filtered, float* History, uint32_t* Pixels, const float* C, int width, int height, arbor_stream stream);
 
+/* Profiling helper (no reference counterpart): counts the traversal and
+ * intersection events one tracePixels (single_tree = 0) or traceTreePixels
+ * (single_tree != 0) launch performs, per thread, into `slots` (caller-owned,
+ * arbor_trace_work_slots(width, height) uint32 values: 16 per thread, events
+ * in the order ray, cell, tree, node, wood, march, bark, wood-shadow, leaf,
+ * newton-start, newton, stone).  It runs the same code compiled with
+ * counters and writes no Hit. */
+ARBOR_API size_t arbor_trace_work_slots(int width, int height);
+ARBOR_API int arbor_traceWork(const float* P, const float* Nodes, const uint32_t* Order, const float* C, int width, int height, int single_tree, uint32_t* slots, arbor_stream stream);
+
 /* ---------------------------------------------------------------------------
  * Engine: the C++ host of src/engine.js (generate / resize / frame /
  * inspect / dispose) over the entries above.
