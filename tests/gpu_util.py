@@ -59,3 +59,10 @@ def ulp_diff(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     ai = np.where(ai < 0, -(ai & 0x7FFFFFFF), ai)
     bi = np.where(bi < 0, -(bi & 0x7FFFFFFF), bi)
     return np.abs(ai - bi)
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """|a - b| / max(1, |b|): absolute error below magnitude 1, relative above."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b) / np.maximum(1.0, np.abs(b))

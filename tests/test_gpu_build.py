@@ -4,9 +4,10 @@ Contract (the reference's own definition of "same scene"):
   - makeKeys, the sort, makeBounds and reduceBounds are bit-exact given the
     same P (they use only + - * / min max);
   - growTree/makePrimitives use sin/cos/pow; the GPU's are correctly rounded
-    and glibc's are not always, so B and P agree within 2 ulp on a few percent
-    of floats, and the Morton keys, order and BVH topology built from the
-    GPU's own P are still bit-exact (checked on every seed below).
+    and glibc's are not always, so a few percent of the floats of B and P
+    differ, by at most 2^-20 relative to max(1, |value|) (about 1e-6 m), and
+    the Morton keys, order and BVH topology built from the GPU's own P are
+    still bit-exact (checked on every seed below).
 """
 import numpy as np
 import pytest
@@ -16,6 +17,7 @@ from conftest import u32
 pytestmark = pytest.mark.gpu
 
 SEEDS = [1, 7, 1788, 42]
+TOL = 2.0 ** -20  # generation floats: |gpu - cpu| <= TOL * max(1, |cpu|)
 
 
 @pytest.fixture(scope="module")
@@ -34,9 +36,9 @@ def test_grow_levels_from_oracle_parents(cuda, oracle, scenes, gu):
         B = gu.dev(before)
         gu.ok(cuda.call("arbor_growTree", B, level, 1788))
         got = gu.host(B)
-        d = gu.ulp_diff(got, B_ref)
-        assert d.max() <= 2, f"level {level}: max ulp {d.max()}"
-        assert np.mean(d > 0) < 0.05
+        e = gu.rel_err(got, B_ref)
+        assert e.max() <= TOL, f"level {level}: max error {e.max()}"
+        assert np.mean(got != B_ref) < 0.05
     assert np.array_equal(B_ref, s["B"])
 
 
@@ -49,8 +51,8 @@ def test_primitives_wood_exact_leaves_close(cuda, oracle, scenes, gu):
     # wood records use no transcendental function: bit-exact
     assert np.array_equal(u32(got[:5124]), u32(want[:5124]))
     assert np.array_equal(u32(got[29412:]), u32(want[29412:]))
-    d = gu.ulp_diff(got, want)
-    assert d.max() <= 2 and np.mean(d > 0) < 0.05
+    assert gu.rel_err(got, want).max() <= TOL
+    assert np.mean(got != want) < 0.05
     assert np.array_equal(got[:, 3], want[:, 3])
 
 
@@ -135,9 +137,9 @@ def test_build_scene_end_to_end(cuda, oracle, gu, seed):
     want = s["Nodes"].reshape(-1, 8)
     assert np.array_equal(nodes[1:, 3], want[1:, 3]), "BVH counts"
     assert np.array_equal(nodes[1:, 7], want[1:, 7]), "leaf ids / internal markers"
-    assert gu.ulp_diff(nodes[1:, [0, 1, 2, 4, 5, 6]], want[1:, [0, 1, 2, 4, 5, 6]]).max() <= 4
+    assert gu.rel_err(nodes[1:, [0, 1, 2, 4, 5, 6]], want[1:, [0, 1, 2, 4, 5, 6]]).max() <= TOL
     P = gu.host(d.P)
-    assert gu.ulp_diff(P, s["P"]).max() <= 2
+    assert gu.rel_err(P, s["P"]).max() <= TOL
     Cw = oracle.init_camera(s["P"], seed)
     assert np.array_equal(u32(gu.host(C)), u32(Cw))
 
@@ -150,7 +152,7 @@ def test_grow_any_level_matches_kernel_semantics(cuda, oracle, scenes, gu):
         oracle.grow(B_ref, level, 1)
         B = gu.dev(s["B"])
         gu.ok(cuda.call("arbor_growTree", B, level, 1))
-        assert gu.ulp_diff(gu.host(B), B_ref).max() <= 2
+        assert gu.rel_err(gu.host(B), B_ref).max() <= TOL
 
 
 def test_sortpass_distance_zero_is_identity(cuda, scenes, gu):
