@@ -543,3 +543,4 @@ extern "C" int arbor_buildScene(int seed, float* B, float* P, uint32_t* Keys, ui
   if (C != nullptr) return arbor_initCamera(C, P, seed, stream);
   return ARBOR_OK;
 }
+

@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "tree"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--width", type=int, default=0, help="override the workload's width (profiling runs)")
+    ap.add_argument("--height", type=int, default=0, help="override the workload's height (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the engine-API end-to-end leg (profiling runs)")
     return ap.parse_args()
 
 
@@ -206,6 +209,8 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
     import arbor_b200 as ab
 
     spec = workload_spec(args.workload)
+    if args.width and args.height:
+        spec.update(width=args.width, height=args.height, workload=spec["workload"] + f" (at {args.width}x{args.height})")
     fr = Frames(ab, spec, torch)
     w, h = fr.w, fr.h
     for k in range(args.warmup):
@@ -278,7 +283,8 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
         pass
 
     # End to end through the engine API with host buffers.
-    result["e2e"] = run_e2e(ab, torch, spec, args)
+    if not args.no_e2e:
+        result["e2e"] = run_e2e(ab, torch, spec, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(spec, args.cpu_seconds)
     if rank == 0:
