@@ -65,6 +65,7 @@ SIGNATURES = {
     "arbor_sort_scratch_bytes": (ctypes.c_size_t, []),
     "arbor_sortKeys": (_i, [_vp, _vp, _vp, _vp]),
     "arbor_buildBounds": (_i, [_vp, _vp, _vp, _vp]),
+    "arbor_sortKeysNoAlloc": (_i, [_vp, _vp, _i, _vp]),
     "arbor_buildScene": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "arbor_traceTreePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_shadeTreePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),

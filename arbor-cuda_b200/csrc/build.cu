@@ -544,3 +544,151 @@ extern "C" int arbor_buildScene(int seed, float* B, float* P, uint32_t* Keys, ui
   return ARBOR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free sort.
+//
+// Some callers cannot allocate device memory: a host that, like the
+// reference's engine (src/engine.js:22,40), owns every buffer and binds only
+// the ABI records to the kernels has no scratch buffer to hand to
+// arbor_sortKeys, and a frame loop running under a fixed memory budget may
+// not call cudaMalloc at all.  arbor_sortKeysNoAlloc sorts the same way as
+// arbor_sortKeys but takes its ping-pong buffer from the file-scope array
+// below, so it allocates nothing.  The array is part of the library image:
+// every GPU that loads the library holds its 256 KB until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace arbor {
+namespace {
+
+constexpr int kNoAllocMaxPairs = kCapacity;  // largest count the array holds
+static __device__ __align__(256) uint32_t g_noalloc_sort_scratch[2 * kNoAllocMaxPairs];
+
+// One 8-bit LSD pass over the first n pairs (n <= kNoAllocMaxPairs), the
+// same stable ranking as radix_pass_kernel with the tail beyond n masked.
+__global__ void __launch_bounds__(kSortThreads) radix_pass_n_kernel(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                                    uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int shift, int n) {
+  __shared__ uint32_t before[256];
+  __shared__ uint32_t total[256];
+  __shared__ uint32_t base[256];
+  __shared__ uint32_t wcnt[kSortThreads / 32][256];
+  const int tid = threadIdx.x;
+  const int start = blockIdx.x * kSortPerCta;
+  if (tid < 256) {
+    before[tid] = 0;
+    total[tid] = 0;
+  }
+  __syncthreads();
+  for (int e = tid; e < n; e += kSortThreads) {
+    uint32_t d = (__ldg(kin + e) >> shift) & 255u;
+    atomicAdd(&total[d], 1u);
+    if (e < start) atomicAdd(&before[d], 1u);
+  }
+  __syncthreads();
+  if (tid < 32) {
+    uint32_t local[8], s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      local[k] = s;
+      s += total[tid * 8 + k];
+    }
+    uint32_t incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (tid >= o) incl += v;
+    }
+    uint32_t excl = incl - s;
+#pragma unroll
+    for (int k = 0; k < 8; k++) base[tid * 8 + k] = excl + local[k] + before[tid * 8 + k];
+  }
+  const int warp = tid >> 5, lane = tid & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int round = 0; round < kSortPerCta / kSortThreads; round++) {
+    for (int k = tid; k < (kSortThreads / 32) * 256; k += kSortThreads) (&wcnt[0][0])[k] = 0;
+    __syncthreads();
+    int e = start + round * kSortThreads + tid;
+    bool live = e < n;
+    uint32_t key = live ? __ldg(kin + e) : 0u, val = live ? __ldg(vin + e) : 0u;
+    uint32_t d = live ? ((key >> shift) & 255u) : 256u;  // 256 marks the masked tail
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t rank = __popc(peers & lt);
+    if (live && rank == 0) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    if (tid < 256) {
+      uint32_t run = base[tid];
+      for (int w = 0; w < kSortThreads / 32; w++) {
+        uint32_t c = wcnt[w][tid];
+        wcnt[w][tid] = run;
+        run += c;
+      }
+      base[tid] = run;
+    }
+    __syncthreads();
+    if (live) {
+      uint32_t pos = wcnt[warp][d] + rank;
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncthreads();
+  }
+}
+
+// Device address of the scratch array, looked up once per device.
+std::mutex g_noalloc_mutex;
+uint32_t* g_noalloc_ptr[64] = {};
+
+int noalloc_scratch(uint32_t** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error("arbor_sortKeysNoAlloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+    return ARBOR_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= 64) {
+    set_error("arbor_sortKeysNoAlloc: device %d is beyond the 64 devices this library tracks", dev);
+    return ARBOR_ERR_LIMIT;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_noalloc_sort_scratch);
+    if (e != cudaSuccess || ptr == nullptr) {
+      set_error("arbor_sortKeysNoAlloc: cudaGetSymbolAddress of the scratch array failed: %s", cudaGetErrorString(e));
+      return ARBOR_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = static_cast<uint32_t*>(ptr);
+  }
+  *out = g_noalloc_ptr[dev];
+  return ARBOR_OK;
+}
+
+}  // namespace
+}  // namespace arbor
+
+extern "C" int arbor_sortKeysNoAlloc(uint32_t* Keys, uint32_t* Order, int count, arbor_stream stream) {
+  const char* name = "arbor_sortKeysNoAlloc";
+  if (count < 0) {
+    set_error("%s: count %d is negative", name, count);
+    return ARBOR_ERR_VALUE;
+  }
+  if (count > kNoAllocMaxPairs) {
+    set_error("%s: count %d exceeds the %d pairs its fixed scratch array holds", name, count, kNoAllocMaxPairs);
+    return ARBOR_ERR_LIMIT;
+  }
+  const Binding b[] = {{Keys, (size_t)count * 4u, true, 4, "Keys"}, {Order, (size_t)count * 4u, true, 4, "Order"}};
+  if (int s = check_bindings(name, b)) return s;
+  if (count == 0) return ARBOR_OK;
+  uint32_t* scratch = nullptr;
+  if (int s = noalloc_scratch(&scratch)) return s;
+  uint32_t* k2 = scratch;
+  uint32_t* v2 = scratch + kNoAllocMaxPairs;
+  int ctas = (count + kSortPerCta - 1) / kSortPerCta;
+  for (int pass = 0; pass < 4; pass++) {
+    bool even = (pass & 1) == 0;
+    radix_pass_n_kernel<<<ctas, kSortThreads, 0, stream>>>(even ? Keys : k2, even ? Order : v2, even ? k2 : Keys, even ? v2 : Order, pass * 8,
+                                                           count);
+  }
+  count_launch(4);
+  return check_launch(name);
+}

@@ -155,6 +155,18 @@ ARBOR_API int arbor_resolvePixels(const float* Filtered, float* History, uint32_
 ARBOR_API size_t arbor_sort_scratch_bytes(void);
 ARBOR_API int arbor_sortKeys(uint32_t* Keys, uint32_t* Order, void* scratch, arbor_stream stream);
 
+/* arbor_sortKeys without a scratch argument, for callers that cannot
+ * allocate device memory (no reference counterpart).  Sorts the first `count`
+ * (Keys, Order) pairs, count <= 32768, in the same order arbor_sortKeys
+ * gives; a larger count returns ARBOR_ERR_LIMIT.  It allocates nothing: its
+ * ping-pong buffer is a fixed 256 KB array inside the library, which every
+ * GPU that loads the library keeps until the process exits.  The first call
+ * on each device looks up that array's device address (cudaGetSymbolAddress),
+ * so make the first call on a device before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (different streams, no
+ * ordering between them) race and corrupt each other's results. */
+ARBOR_API int arbor_sortKeysNoAlloc(uint32_t* Keys, uint32_t* Order, int count, arbor_stream stream);
+
 /* Makes leaf nodes (as makeBounds) and all 15 parent levels (as the 15
  * reduceBounds dispatches, src/engine.js:32) in two launches. */
 ARBOR_API int arbor_buildBounds(const float* P, const uint32_t* Order, float* Nodes, arbor_stream stream);
