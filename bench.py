@@ -346,48 +346,58 @@ def cpu_oracle():
     return Oracle("port"), "port"
 
 
+class CpuFrame:
+    """The workload's first frame on the CPU implementation, rendered on an
+    evenly strided subset of its rows (a representative sample of the frame;
+    each pass is one OpenMP loop over the sampled rows)."""
+
+    def __init__(self, o, spec: dict):
+        import workloads
+
+        self.o, self.spec = o, spec
+        w, h, seed = spec["width"], spec["height"], spec["seed"]
+        self.scene = o.build_scene(seed)
+        if spec["single_tree"]:
+            C = workloads.single_tree_camera(w, h, seed)
+        else:
+            C = o.init_camera(self.scene["P"], seed)
+            C[22] = 1.0 if spec["shadows"] else 0.0
+            if spec["shadows"]:
+                C[12], C[13] = workloads.shadow_sun(seed)
+            I, dt = workloads.walk_input(0, seed)
+            o.update_camera(C, I, self.scene["P"], dt, w, h)
+        self.C = C
+        self.bufs = {k: np.zeros(w * h * 4, np.float32) for k in ("Hit", "Linear", "Guide", "Filtered", "History")}
+        self.bufs["Pixels"] = np.zeros(w * h, np.uint32)
+
+    def rows(self, n: int) -> np.ndarray:
+        h = self.spec["height"]
+        n = max(1, min(n, h))
+        return np.unique((np.arange(n) * h // n + (h // n) // 2).clip(0, h - 1)).astype(np.int32)
+
+    def render(self, n: int) -> tuple[int, float, int]:
+        rows = self.rows(n)
+        t0 = time.perf_counter()
+        self.o.frame_rows(self.scene, self.C, self.spec["width"], self.spec["height"], rows, self.bufs, single=self.spec["single_tree"])
+        secs = time.perf_counter() - t0
+        return len(rows) * self.spec["width"] * self.spec["spp"], secs, len(rows)
+
+    def calibrate(self, target_s: float) -> int:
+        """Number of sampled rows for about target_s seconds (at least 4 per host thread)."""
+        h = self.spec["height"]
+        n = min(h, 4 * max(1, self.o.max_threads()))
+        _, secs, n = self.render(n)
+        return int(min(h, max(n, n * target_s / max(secs, 1e-3))))
+
+
 def cpu_sample(o, kind: str, spec: dict, target_s: float) -> dict:
-    """Time the CPU render of a band of rows of the workload's first frame."""
-    import workloads
-
-    w, h, seed = spec["width"], spec["height"], spec["seed"]
-    scene = o.build_scene(seed)
-    if spec["single_tree"]:
-        C = workloads.single_tree_camera(w, h, seed)
-    else:
-        C = o.init_camera(scene["P"], seed)
-        C[22] = 1.0 if spec["shadows"] else 0.0
-        if spec["shadows"]:
-            C[12], C[13] = workloads.shadow_sun(seed)
-        I, dt = workloads.walk_input(0, seed)
-        o.update_camera(C, I, scene["P"], dt, w, h)
-    single = spec["single_tree"]
-    bufs = {k: np.zeros(w * h * 4, np.float32) for k in ("Hit", "Linear", "Guide", "Filtered", "History")}
-    pixels = np.zeros(w * h, np.uint32)
-
-    def band(y0, y1):
-        o.trace(scene, C, w, h, y0, y1, single=single, Hit=bufs["Hit"])
-        o.shade(scene, C, bufs["Hit"], w, h, y0, y1, single=single, Linear=bufs["Linear"], Guide=bufs["Guide"])
-        o.filter(bufs["Linear"], bufs["Guide"], bufs["Hit"], C, w, h, y0, y1, Filtered=bufs["Filtered"])
-        o.resolve(bufs["Filtered"], bufs["History"], C, w, h, y0, y1, Pixels=pixels)
-
-    # Calibrate on a small band around the horizon (the busiest rows), then
-    # size the sample to about target_s seconds.
-    mid = h // 2
-    rows = max(2, h // 64)
-    t0 = time.perf_counter()
-    band(mid - rows // 2, mid - rows // 2 + rows)
-    dt = time.perf_counter() - t0
-    rows = int(min(h, max(rows, rows * target_s / max(dt, 1e-3))))
-    y0 = max(0, mid - rows // 2)
-    y1 = min(h, y0 + rows)
-    t0 = time.perf_counter()
-    band(y0, y1)
-    secs = time.perf_counter() - t0
-    rays = (y1 - y0) * w * spec["spp"]
+    frame = CpuFrame(o, spec)
+    n = frame.calibrate(target_s)
+    rays, secs, n = frame.render(n)
     return {"value": round(rays / secs / 1e6, 4), "unit": UNIT, "cores": o.max_threads(), "kind": kind,
-            "sample": f"rows {y0}..{y1 - 1} of frame 0 ({rays} primary rays, {secs:.2f} s): trace, shade, filter, resolve",
-            "seconds": round(secs, 3), "rows": y1 - y0}
+            "sample": f"{n} evenly strided rows of {spec['height']} of frame 0 ({rays} primary rays, {secs:.2f} s): "
+                      "trace, shade, filter, resolve",
+            "seconds": round(secs, 3)}
 
 
 def cpu_baseline(spec: dict, target_s: float) -> dict:
@@ -399,61 +409,29 @@ def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
     spec = workload_spec(args.workload)
+    if args.width and args.height:
+        spec.update(width=args.width, height=args.height)
     o, kind = cpu_oracle()
-    # Each step is a band of rows sized to about 2 s, so that warmup + steps
-    # finish within a few minutes.
-    per_step_s = float(os.environ.get("ARBOR_REFERENCE_STEP_SECONDS", "2.0"))
-    first = cpu_sample(o, kind, spec, per_step_s)
-    rows = first["rows"]
-    w, h = spec["width"], spec["height"]
-    rates = []
+    frame = CpuFrame(o, spec)
+    # Each step renders the same evenly spaced bands, sized to about 2 s, so
+    # that warmup + steps finish within a few minutes.
+    n = frame.calibrate(float(os.environ.get("ARBOR_REFERENCE_STEP_SECONDS", "2.0")))
+    times, rays = [], 0
     for k in range(args.warmup + args.steps):
-        s = cpu_sample_fixed(o, spec, rows, k)
+        rays, secs, n = frame.render(n)
         if k >= args.warmup:
-            rates.append(s)
-    rays = rows * w * spec["spp"]
-    total_s = sum(rates)
-    value = rays * len(rates) / total_s / 1e6
+            times.append(secs)
+    total_s = sum(times)
+    value = rays * len(times) / total_s / 1e6
     line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(total_s * 1e3 / len(rates), 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": round(total_s * 1e3 / len(times), 2), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic: procedural scene grown from the master seed", "impl": "reference",
-            "config": {**spec, "sample_rows": rows},
+            "config": {**spec, "sample_rows": n},
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": o.max_threads(), "kind": kind,
-                             "sample": f"each step renders {rows} of {h} rows of frame 0 ({rays} primary rays): trace, shade, filter, resolve"},
+                             "sample": f"each step renders {n} evenly strided rows of {spec['height']} of frame 0 "
+                                       f"({rays} primary rays): trace, shade, filter, resolve"},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-_CPU_STATE = {}
-
-
-def cpu_sample_fixed(o, spec: dict, rows: int, k: int) -> float:
-    import workloads
-
-    w, h, seed = spec["width"], spec["height"], spec["seed"]
-    if "scene" not in _CPU_STATE:
-        scene = o.build_scene(seed)
-        if spec["single_tree"]:
-            C = workloads.single_tree_camera(w, h, seed)
-        else:
-            C = o.init_camera(scene["P"], seed)
-            C[22] = 1.0 if spec["shadows"] else 0.0
-            if spec["shadows"]:
-                C[12], C[13] = workloads.shadow_sun(seed)
-            I, dt = workloads.walk_input(0, seed)
-            o.update_camera(C, I, scene["P"], dt, w, h)
-        _CPU_STATE.update(scene=scene, C=C, bufs={n: np.zeros(w * h * 4, np.float32) for n in ("Hit", "Linear", "Guide", "Filtered", "History")},
-                          pixels=np.zeros(w * h, np.uint32))
-    scene, C, b = _CPU_STATE["scene"], _CPU_STATE["C"], _CPU_STATE["bufs"]
-    single = spec["single_tree"]
-    y0 = max(0, h // 2 - rows // 2)
-    y1 = min(h, y0 + rows)
-    t0 = time.perf_counter()
-    o.trace(scene, C, w, h, y0, y1, single=single, Hit=b["Hit"])
-    o.shade(scene, C, b["Hit"], w, h, y0, y1, single=single, Linear=b["Linear"], Guide=b["Guide"])
-    o.filter(b["Linear"], b["Guide"], b["Hit"], C, w, h, y0, y1, Filtered=b["Filtered"])
-    o.resolve(b["Filtered"], b["History"], C, w, h, y0, y1, Pixels=_CPU_STATE["pixels"])
-    return time.perf_counter() - t0
 
 
 def main() -> None:

@@ -1073,3 +1073,21 @@ EXPORT void oracle_leafPair(const float* P, int k, float* out) {
   out[0] = (float)leaf_hit(P, id, p, rd, 0.00001f, 0.0f, 0.0f);
   out[1] = (float)leaf_hit(P, id, p, rd, 0.05f, 0.0f, 0.0f);
 }
+/* One frame (trace, shade, filter, resolve) over a list of rows: each pass is
+ * one OpenMP loop over the listed rows with the harness's schedule, so a
+ * sample of rows spread over the image keeps every host thread busy. */
+EXPORT void oracle_frameRows(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, float* Linear, float* Guide,
+                             float* Filtered, float* History, uint32_t* Pixels, int w, int h, const int* rows, int n, int single) {
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < n; i++)
+    for (int x = 0; x < w; x++) trace_px(P, Nodes, Order, C, Hit, w, h, x, rows[i], single);
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < n; i++)
+    for (int x = 0; x < w; x++) shade_px(P, Nodes, Order, C, Hit, Linear, Guide, w, h, x, rows[i], single);
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < n; i++)
+    for (int x = 0; x < w; x++) filter_px(Linear, Guide, Hit, Filtered, C, w, h, x, rows[i]);
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < n; i++)
+    for (int x = 0; x < w; x++) resolve_px(Filtered, History, Pixels, C, w, h, x, rows[i]);
+}

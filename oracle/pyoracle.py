@@ -68,6 +68,7 @@ _SIGNATURES = {
     "oracle_harnessRay": (None, [_c_int, _f, _f]),
     "oracle_footprintSweep": (None, [_f, _c_int, _f]),
     "oracle_leafPair": (None, [_f, _c_int, _f]),
+    "oracle_frameRows": (None, [_f, _f, _u, _f, _f, _f, _f, _f, _f, _u, _c_int, _c_int, _i, _c_int, _c_int]),
 }
 _OPTIONAL = {
     # only in the reference build: the harness's Renderer constructor
@@ -241,6 +242,13 @@ class Oracle:
         Filtered = self.filter(Linear, Guide, Hit, C, w, h)
         Pixels = self.resolve(Filtered, History, C, w, h)
         return {"Hit": Hit, "Linear": Linear, "Guide": Guide, "Filtered": Filtered, "History": History, "Pixels": Pixels}
+
+    def frame_rows(self, scene, C, w, h, rows, bufs: dict, single=False) -> None:
+        """trace, shade, filter, resolve over the listed rows only (into bufs)."""
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        self.lib.oracle_frameRows(_p(scene["P"]), _p(scene["Nodes"]), _p(scene["Order"]), _p(C), _p(bufs["Hit"]), _p(bufs["Linear"]),
+                                  _p(bufs["Guide"]), _p(bufs["Filtered"]), _p(bufs["History"]), _p(bufs["Pixels"]), w, h, _p(rows),
+                                  len(rows), int(single))
 
     def trace_pixel_list(self, scene, C, w, h, xy: np.ndarray, single=False) -> np.ndarray:
         """Trace only the listed (x, y) pixels; returns a full-size Hit with the rest zero."""

@@ -240,3 +240,27 @@ EXPORT void oracle_leafPair(const float* P, int k, float* out) {
   auto p = read3(P, b) + u * (P[b + 16] + P[b + 7] * .5f) + n * .10f; auto rd = n * -1.0f;
   out[0] = leafT(P, id, p, rd, .00001f, 0, 0); out[1] = leafT(P, id, p, rd, .05f, 0, 0);
 }
+namespace {
+template <class F> void each_listed_row(int w, const int* rows, int n, F f) {
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < n; i++)
+    for (int x = 0; x < w; x++) {
+      int y = rows[i];
+      blockDim = {8, 8, 1};
+      blockIdx = {unsigned(x / 8), unsigned(y / 8), 0};
+      threadIdx = {unsigned(x % 8), unsigned(y % 8), 0};
+      f(x, y);
+    }
+}
+}  // namespace
+EXPORT void oracle_frameRows(const float* P, const float* Nodes, const unsigned* Order, const float* C, float* Hit, float* Linear, float* Guide,
+                             float* Filtered, float* History, unsigned* Pixels, int w, int h, const int* rows, int n, int single) {
+  each_listed_row(w, rows, n, [&](int x, int y) {
+    if (single) trace_single(P, Nodes, Order, C, Hit, w, h, x, y); else tracePixels(P, Nodes, Order, C, Hit, w, h);
+  });
+  each_listed_row(w, rows, n, [&](int x, int y) {
+    if (single) shade_single(P, Nodes, Order, C, Hit, Linear, Guide, w, h, x, y); else shadePixels(P, Nodes, Order, C, Hit, Linear, Guide, w, h);
+  });
+  each_listed_row(w, rows, n, [&](int, int) { filterLighting(Linear, Guide, Hit, Filtered, C, w, h); });
+  each_listed_row(w, rows, n, [&](int, int) { resolvePixels(Filtered, History, Pixels, C, w, h); });
+}
