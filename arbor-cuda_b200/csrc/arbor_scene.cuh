@@ -175,6 +175,14 @@ __device__ __forceinline__ Leaf load_leaf(const float* P, int id, float time, fl
   l.stem = r4.x;
   l.curl = r4.y;
   l.twist = r4.z;
+  if (wind == 0.0f) {
+    // Still air: the rotation angle is wind * (finite) = +-0, so cos = 1 and
+    // sin = +-0 and the reference's u*cos + n*sin, n*cos - u*sin are u and n
+    // exactly (up to the sign of a zero component).
+    l.u = u;
+    l.n = n;
+    return l;
+  }
   float phase = (float)(l.seed % 8192) * 0.618f;
   float a = wind * (0.11f * sinf(time * 2.1f + phase) + 0.045f * sinf(time * 5.8f + phase * 1.7f));
   float ca = cosf(a), sa = sinf(a);
@@ -274,45 +282,74 @@ static __device__ __noinline__ float wood_t(const float* P, int id, f3 ro, f3 rd
   }
   return kFar;
 }
-// Curved-leaf Newton solve (Arbor.cu:203-218).
-static __device__ __noinline__ float leaf_t(const float* P, int id, f3 ro, f3 rd, float footprint, float time, float wind) {
+// Curved-leaf intersection (Arbor.cu:203-218), in two parts so the
+// wavefront tracer can run them as separate compacted stages: leaf_clip does
+// the frame, the petiole tube and the leaf-box clip; leaf_newton does the
+// seven Newton steps and the acceptance test.  leaf_t chains them and is the
+// reference's leafT.
+struct LeafSolve {
+  float x, y, z, dx, dy, dz;  // ray in the leaf frame
+  float t, spanx, spany;      // Newton start and the clipped interval
+  float best;                 // petiole tube result
+  float len, width, curl, twist;
+};
+// Returns true when the leaf box is hit and the Newton solve must run;
+// otherwise the result is s.best.
+__device__ __forceinline__ bool leaf_clip(const float* P, int id, f3 ro, f3 rd, float time, float wind, LeafSolve& s) {
   ARBOR_COUNT(kEvLeaf);
   Leaf l = load_leaf(P, id, time, wind);
   f3 q = ro - l.origin;
-  float x = dot3(q, l.u) - l.stem;
-  float y = dot3(q, l.v);
-  float z = dot3(q, l.n);
-  float dx = dot3(rd, l.u);
-  float dy = dot3(rd, l.v);
-  float dz = dot3(rd, l.n);
-  float best = tube_t(ro, rd, l.origin, l.origin + l.u * l.stem, 0.0011f, 0.00065f);
-  f2 span = box_span(mk(x, y, z), mk(dx, dy, dz), mk(-0.001f, -l.width, -0.035f), mk(l.len + 0.001f, l.width, 0.065f));
-  if (span.y < fmaxf(0.0001f, span.x)) return best;
+  s.x = dot3(q, l.u) - l.stem;
+  s.y = dot3(q, l.v);
+  s.z = dot3(q, l.n);
+  s.dx = dot3(rd, l.u);
+  s.dy = dot3(rd, l.v);
+  s.dz = dot3(rd, l.n);
+  s.best = tube_t(ro, rd, l.origin, l.origin + l.u * l.stem, 0.0011f, 0.00065f);
+  f2 span = box_span(mk(s.x, s.y, s.z), mk(s.dx, s.dy, s.dz), mk(-0.001f, -l.width, -0.035f), mk(l.len + 0.001f, l.width, 0.065f));
+  if (span.y < fmaxf(0.0001f, span.x)) return false;
   ARBOR_COUNT(kEvNewtonStart);
-  float t = fabsf(dz) > 0.000001f ? -z / dz : (span.x + span.y) * 0.5f;
-  t = clampf(t, fmaxf(0.0001f, span.x), span.y);
-  float hw2 = l.width * l.width;
+  float t = fabsf(s.dz) > 0.000001f ? -s.z / s.dz : (span.x + span.y) * 0.5f;
+  s.t = clampf(t, fmaxf(0.0001f, span.x), span.y);
+  s.spanx = span.x;
+  s.spany = span.y;
+  s.len = l.len;
+  s.width = l.width;
+  s.curl = l.curl;
+  s.twist = l.twist;
+  return true;
+}
+__device__ __forceinline__ float leaf_newton(const LeafSolve& s, float footprint) {
+  const float x = s.x, y = s.y, z = s.z, dx = s.dx, dy = s.dy, dz = s.dz;
+  float t = s.t;
+  float best = s.best;
+  float hw2 = s.width * s.width;
   float bw007 = band_weight(0.007f, footprint);
   for (int k = 0; k < 7; k++) {
     ARBOR_COUNT(kEvNewton);
     float xx = x + dx * t;
     float yy = y + dy * t;
-    float height = leaf_height(xx, yy, l.len, hw2, l.curl, l.twist, bw007);
+    float height = leaf_height(xx, yy, s.len, hw2, s.curl, s.twist, bw007);
     float f = z + dz * t - height;
     const float e = 0.00015f;
-    float hx = (leaf_height(xx + e, yy, l.len, hw2, l.curl, l.twist, bw007) - leaf_height(xx - e, yy, l.len, hw2, l.curl, l.twist, bw007)) / (2.0f * e);
-    float hy = (leaf_height(xx, yy + e, l.len, hw2, l.curl, l.twist, bw007) - leaf_height(xx, yy - e, l.len, hw2, l.curl, l.twist, bw007)) / (2.0f * e);
+    float hx = (leaf_height(xx + e, yy, s.len, hw2, s.curl, s.twist, bw007) - leaf_height(xx - e, yy, s.len, hw2, s.curl, s.twist, bw007)) / (2.0f * e);
+    float hy = (leaf_height(xx, yy + e, s.len, hw2, s.curl, s.twist, bw007) - leaf_height(xx, yy - e, s.len, hw2, s.curl, s.twist, bw007)) / (2.0f * e);
     float deriv = dz - hx * dx - hy * dy;
     if (fabsf(deriv) < 0.00001f) break;
     t -= clampf(f / deriv, -0.13f, 0.13f);
-    t = clampf(t, span.x, span.y);
+    t = clampf(t, s.spanx, s.spany);
   }
   float xx = x + dx * t;
   float yy = y + dy * t;
-  float err = fabsf(z + dz * t - leaf_height(xx, yy, l.len, hw2, l.curl, l.twist, bw007));
-  if (t > 0.0001f && xx > 0.0f && xx < l.len && err < 0.0003f && fabsf(yy) < leaf_width(xx, l.len, l.width, band_weight(0.002f, footprint)))
+  float err = fabsf(z + dz * t - leaf_height(xx, yy, s.len, hw2, s.curl, s.twist, bw007));
+  if (t > 0.0001f && xx > 0.0f && xx < s.len && err < 0.0003f && fabsf(yy) < leaf_width(xx, s.len, s.width, band_weight(0.002f, footprint)))
     best = fminf(best, t);
   return best;
+}
+static __device__ __noinline__ float leaf_t(const float* P, int id, f3 ro, f3 rd, float footprint, float time, float wind) {
+  LeafSolve s;
+  if (!leaf_clip(P, id, ro, rd, time, wind, s)) return s.best;
+  return leaf_newton(s, footprint);
 }
 // Arbor.cu:219
 __device__ __forceinline__ float object_t(const float* P, int id, f3 ro, f3 rd, float footprint, float time, float wind, bool refine) {

@@ -15,7 +15,7 @@ namespace {
 
 // ---------------------------------------------------------------- trace --
 template <bool kForestScene>
-__global__ void __launch_bounds__(kBlock) trace_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+__global__ void __launch_bounds__(kBlock, 3) trace_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                        const uint32_t* __restrict__ Order, const float* __restrict__ C,
                                                        float* __restrict__ Hit, int width, int height) {
   __shared__ Camera cam;
