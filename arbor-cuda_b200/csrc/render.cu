@@ -14,29 +14,58 @@ namespace arbor {
 namespace {
 
 // ---------------------------------------------------------------- trace --
+// One ray per thread over 16x16-pixel CTAs (8x4-pixel warps); each warp's
+// primitive tests run warp-batched (warpbatch.cuh).
+struct PrimaryPolicy {
+  const Camera* cam;
+  float* Hit;
+  int width, height, pixel;
+  __device__ __forceinline__ void done(Ray& r) {
+    reinterpret_cast<float4*>(Hit)[pixel] = make_float4(r.best, r.found, (float)r.foundTree, cam->c14 * r.best / (float)height);
+    r.phase = kPhIdle;
+  }
+};
+
 template <bool kForestScene>
-__global__ void __launch_bounds__(kBlock, 3) trace_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
-                                                       const uint32_t* __restrict__ Order, const float* __restrict__ C,
-                                                       float* __restrict__ Hit, int width, int height) {
+__global__ void __launch_bounds__(kBlock, 2) trace_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                          const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                          float* __restrict__ Hit, int width, int height) {
+  extern __shared__ float4 batch_smem[];
+  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
   __shared__ Camera cam;
   __shared__ Instance inst[kForestScene ? kForest : 1];
   block_setup(C, cam, inst, kForestScene);
+  const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, kForestScene};
   int x, y;
   tile_pixel(threadIdx.x, x, y);
-  if (x >= width || y >= height) return;
-  f3 ro = cam.ro;
-  f3 rd = camera_ray(cam, x, y, width, height);
-  float ground = rd.y < -0.00001f ? -ro.y / rd.y : kFar;
-  float cone = cam.c14 / (float)height;
-  float best = ground > 0.0f ? ground : kFar;
-  int tree = -1;
-  f2 h;
-  if (kForestScene) {
-    h = trace_forest(P, Nodes, Order, inst, ro, rd, cone, cam.time, cam.wind, best, &tree, false);
-  } else {
-    h = trace_tree(P, Nodes, Order, ro, rd, cone, cam.time, cam.wind, best, -1, false);
+  PrimaryPolicy policy{&cam, Hit, width, height, y * width + x};
+  Ray r;
+  r.phase = kPhIdle;
+  if (x < width && y < height) {
+    f3 rd = camera_ray(cam, x, y, width, height);
+    float ground = rd.y < -0.00001f ? -cam.ro.y / rd.y : kFar;  // Arbor.cu:252
+    ray_begin(c, r, cam.ro, rd, ground > 0.0f ? ground : kFar);
   }
-  reinterpret_cast<float4*>(Hit)[y * width + x] = make_float4(h.x, h.y, (float)tree, cam.c14 * h.x / (float)height);
+  batch_run(c, r, b, policy);
+}
+
+// Dynamic shared memory of a 256-thread CTA: one WarpBatch per warp.
+constexpr size_t kBatchSmem = sizeof(WarpBatch) * (kBlock / 32);
+
+// Opt a kernel in to kBatchSmem of dynamic shared memory, once per device.
+inline bool batch_smem_ready(const void* kernel) {
+  static const void* done[64][8] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  for (int i = 0; i < 8; i++) {
+    if (done[dev][i] == kernel) return true;
+    if (done[dev][i] == nullptr) {
+      if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem) != cudaSuccess) return false;
+      done[dev][i] = kernel;
+      return true;
+    }
+  }
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem) == cudaSuccess;
 }
 
 // ---------------------------------------------------------------- shade --
@@ -157,27 +186,6 @@ __device__ f3 surface_color(const float* P, int id, f3 p, float fp, float time, 
   float f = noise3(p * 42.0f, (int)ldg4(P, id * 6 + 3).w);
   return mix3(mk(0.09f, 0.10f, 0.086f), mk(0.31f, 0.30f, 0.24f), f);
 }
-// Sun visibility through at most four segments (Arbor.cu:271-274).
-template <bool kForestScene>
-__device__ f3 light_visibility(const float* P, const float* Nodes, const uint32_t* Order, const Instance* inst, f3 p, f3 direction, float time,
-                               float wind) {
-  f3 transmission = mk(1.0f, 1.0f, 1.0f);
-  f3 ro = p;
-  for (int j = 0; j < 4; j++) {
-    int tree = -1;
-    f2 h;
-    if (kForestScene)
-      h = trace_forest(P, Nodes, Order, inst, ro, direction, 0.0001f, time, wind, 36.0f, &tree, true);
-    else
-      h = trace_tree(P, Nodes, Order, ro, direction, 0.0001f, time, wind, 36.0f, -1, true);
-    int id = (int)h.y;
-    if (id < 0) break;
-    if (ldg4(P, id * 6).w != 1.0f) return mk(0.0f, 0.0f, 0.0f);
-    transmission = transmission * mk(0.18f, 0.29f, 0.065f);
-    ro = ro + direction * (h.x + 0.0018f);
-  }
-  return transmission;
-}
 // Arbor.cu:276
 __device__ float spec_ggx(f3 n, f3 v, f3 l, float rough) {
   f3 h = norm3(v + l);
@@ -195,21 +203,24 @@ __device__ float spec_ggx(f3 n, f3 v, f3 l, float rough) {
   return D * G * F / (4.0f * nv + 0.0001f);
 }
 
-// One pixel of shadePixels (Arbor.cu:277-289).  The single-tree scene uses
-// the identity instance: tree-local point and normal, phase 0, no tint.
+// shadePixels (Arbor.cu:277-289) is split at the sun-visibility call:
+// shade_pre computes everything before it, the shadow segments are traced by
+// the warp tracer, shade_post composes the colour.  Each value is computed
+// with the reference's operations in the reference's order; the colour
+// before haze is (direct * visibility) * (4.8, 4.2, 3.1) + albedo * ambient.
+struct Shading {
+  f3 direct, ambientTerm, skyc, guide, origin, light, debug;
+  float haze;
+  bool final;   // colour is `debug` (sky pixel or debug view mode): no visibility needed
+  bool shadow;  // visibility must be traced
+};
+
+// The single-tree scene uses the identity instance: tree-local point and
+// normal, phase 0, no tint.
 template <bool kForestScene>
-__global__ void __launch_bounds__(kBlock) shade_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
-                                                       const uint32_t* __restrict__ Order, const float* __restrict__ C,
-                                                       const float* __restrict__ Hit, float* __restrict__ Linear,
-                                                       float* __restrict__ Guide, int width, int height) {
-  __shared__ Camera cam;
-  __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
-  int x, y;
-  tile_pixel(threadIdx.x, x, y);
-  if (x >= width || y >= height) return;
+__device__ __noinline__ void shade_pre(const float* P, const Camera& cam, const Instance* inst, float4 hit, int x, int y, int width, int height,
+                          Shading& o) {
   int pixel = y * width + x;
-  float4 hit = __ldg(reinterpret_cast<const float4*>(Hit) + pixel);
   float t = hit.x;
   int id = (int)hit.y;
   int tree = (int)hit.z;
@@ -220,91 +231,174 @@ __global__ void __launch_bounds__(kBlock) shade_kernel(const float* __restrict__
   f3 ro = cam.ro;
   f3 rd = camera_ray(cam, x, y, width, height);
   f3 sun = cam.sun;
-  f3 col = sky(rd, sun);
-  f3 guide = mk(1.0f, 1.0f, 1.0f);
-  if (t < kFar) {
-    f3 p = ro + rd * t;
-    float fp = fmaxf(0.000005f, hit.w);
-    f3 localP = p;
-    f3 n = mk(0.0f, 1.0f, 0.0f);
-    float localFp = fp;
-    float phase = 0.0f;
-    const float time = cam.time, wind = cam.wind;
-    if (kForestScene) {
-      if (id >= 0 && tree >= 0) {
-        const Instance& it = inst[tree];
-        localP = to_local_point(p, it);
-        localFp = fp / it.sc;
-        phase = it.phase;
-        n = to_world_normal(object_normal(P, id, localP, localFp, time + phase, wind), it);
-      }
-    } else if (id >= 0) {
-      n = object_normal(P, id, localP, localFp, time, wind);
+  o.skyc = sky(rd, sun);
+  o.guide = mk(1.0f, 1.0f, 1.0f);
+  o.shadow = false;
+  if (!(t < kFar)) {
+    o.final = true;
+    o.debug = o.skyc;
+    return;
+  }
+  f3 p = ro + rd * t;
+  float fp = fmaxf(0.000005f, hit.w);
+  f3 localP = p;
+  f3 n = mk(0.0f, 1.0f, 0.0f);
+  float localFp = fp;
+  float phase = 0.0f;
+  const float time = cam.time, wind = cam.wind;
+  if (kForestScene) {
+    if (id >= 0 && tree >= 0) {
+      const Instance& it = inst[tree];
+      localP = to_local_point(p, it);
+      localFp = fp / it.sc;
+      phase = it.phase;
+      n = to_world_normal(object_normal(P, id, localP, localFp, time + phase, wind), it);
     }
-    bool leaf = id >= 0 && ldg4(P, id * 6).w == 1.0f;
-    if (dot3(n, rd) > 0.0f) n = n * -1.0f;
-    if (id < 0) {
-      float e = fmaxf(0.001f, fp);
-      uint32_t h133 = hashU(133u);
-      float nx = (noise_h((p.x + e) * 18.0f, p.z * 18.0f, h133) - noise_h((p.x - e) * 18.0f, p.z * 18.0f, h133)) * 0.18f;
-      float nz = (noise_h(p.x * 18.0f, (p.z + e) * 18.0f, h133) - noise_h(p.x * 18.0f, (p.z - e) * 18.0f, h133)) * 0.18f;
-      n = norm3(mk(nx, 1.0f, nz));
-    }
-    f3 albedo = surface_color(P, id, id >= 0 ? localP : p, localFp, time + phase, wind);
-    if (kForestScene && tree >= 0) {
-      int ts = inst[tree].seed;
-      float hue = rnd(8, ts);
-      float age = rnd(9, ts);
-      float season = rnd(10, ts);
-      float dark = 0.76f + age * 0.38f;
-      f3 tint = mk(0.88f + 0.22f * hue, 0.84f + 0.28f * (1.0f - fabsf(hue - 0.55f)), 0.72f + 0.25f * (1.0f - hue));
-      if (leaf)
-        tint = mix3(tint, mk(1.12f, 0.88f, 0.48f), smooth(0.78f, 0.98f, season) * 0.38f);
-      else
-        tint = mix3(tint, mk(0.78f, 0.66f, 0.53f), season * 0.18f);
-      albedo = albedo * tint * dark;
-    }
-    guide = albedo;
-    int sample = cam.sample;
-    float r1 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 1823u), 991);
-    float r2 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 971u), 731);
-    f3 su = basisU(sun);
-    f3 sv = cross3(sun, su);
-    float angle = r1 * 6.28318f;
-    float disk = sqrtf(r2) * 0.012f;
-    f3 light = norm3(sun + su * (xcos(angle) * disk) + sv * (xsin(angle) * disk));
-    float offset = id >= 0 ? 0.0014f : 0.004f;
-    f3 visibility = mk(1.0f, 1.0f, 1.0f);
-    if (cam.shadows > 0.5f) visibility = light_visibility<kForestScene>(P, Nodes, Order, inst, p + light * offset, light, time, wind);
-    float nl = sat(dot3(n, light));
-    float back = sat(-dot3(n, light));
-    f3 direct = albedo * (nl / kPi);
-    if (leaf) {
-      float vein = leaf_vein(load_leaf(P, id, time + phase, wind), localP, localFp);
-      direct = direct + albedo * (back * (0.75f - 0.25f * vein) + xpow(sat(dot3(rd, light)), 9.0f) * 0.12f);
-    }
-    float spec = spec_ggx(n, rd * -1.0f, light, leaf ? 0.39f : 0.82f);
-    direct = direct + mk(spec, spec, spec);
-    float ao = 1.0f;
-    f3 ambient = mk(0.30f, 0.37f, 0.45f) * (0.45f + 0.55f * sat(n.y)) * ao + mk(0.08f, 0.068f, 0.035f) * sat(-n.y);
-    if (leaf) ambient = ambient + mk(0.04f, 0.055f, 0.022f) * ao;
-    col = direct * visibility * mk(4.8f, 4.2f, 3.1f) + albedo * ambient;
-    float haze = 1.0f - xexp(-t * 0.0018f);
-    col = mix3(col, sky(rd, sun), haze);
+  } else if (id >= 0) {
+    n = object_normal(P, id, localP, localFp, time, wind);
+  }
+  bool leaf = id >= 0 && ldg4(P, id * 6).w == 1.0f;
+  if (dot3(n, rd) > 0.0f) n = n * -1.0f;
+  if (id < 0) {
+    float e = fmaxf(0.001f, fp);
+    uint32_t h133 = hashU(133u);
+    float nx = (noise_h((p.x + e) * 18.0f, p.z * 18.0f, h133) - noise_h((p.x - e) * 18.0f, p.z * 18.0f, h133)) * 0.18f;
+    float nz = (noise_h(p.x * 18.0f, (p.z + e) * 18.0f, h133) - noise_h(p.x * 18.0f, (p.z - e) * 18.0f, h133)) * 0.18f;
+    n = norm3(mk(nx, 1.0f, nz));
+  }
+  f3 albedo = surface_color(P, id, id >= 0 ? localP : p, localFp, time + phase, wind);
+  if (kForestScene && tree >= 0) {
+    int ts = inst[tree].seed;
+    float hue = rnd(8, ts);
+    float age = rnd(9, ts);
+    float season = rnd(10, ts);
+    float dark = 0.76f + age * 0.38f;
+    f3 tint = mk(0.88f + 0.22f * hue, 0.84f + 0.28f * (1.0f - fabsf(hue - 0.55f)), 0.72f + 0.25f * (1.0f - hue));
+    if (leaf)
+      tint = mix3(tint, mk(1.12f, 0.88f, 0.48f), smooth(0.78f, 0.98f, season) * 0.38f);
+    else
+      tint = mix3(tint, mk(0.78f, 0.66f, 0.53f), season * 0.18f);
+    albedo = albedo * tint * dark;
+  }
+  o.guide = albedo;
+  if (cam.mode == 1.0f || cam.mode == 2.0f || cam.mode == 3.0f) {
+    // Debug views replace the colour whatever the lighting (Arbor.cu:286).
+    o.final = true;
     if (cam.mode == 1.0f) {
       float w0 = band_weight(0.065f, localFp);
       float w1 = band_weight(0.005f, localFp);
       float w2 = band_weight(0.001f, localFp);
-      col = mk(w0 * 0.80f, w1 * 0.85f, w2 * 0.9f);
-    }
-    if (cam.mode == 2.0f) {
+      o.debug = mk(w0 * 0.80f, w1 * 0.85f, w2 * 0.9f);
+    } else if (cam.mode == 2.0f) {
       float hh = rnd(id + 177 + (tree + 1) * 71, 32);
-      col = id < 0 ? mk(0.10f, 0.10f, 0.10f) : (leaf ? mk(0.1f, 0.3f + hh * 0.5f, 0.17f) : mk(0.47f + hh * 0.3f, 0.25f, 0.10f));
+      o.debug = id < 0 ? mk(0.10f, 0.10f, 0.10f) : (leaf ? mk(0.1f, 0.3f + hh * 0.5f, 0.17f) : mk(0.47f + hh * 0.3f, 0.25f, 0.10f));
+    } else {
+      o.debug = n * 0.5f + mk(0.5f, 0.5f, 0.5f);
     }
-    if (cam.mode == 3.0f) col = n * 0.5f + mk(0.5f, 0.5f, 0.5f);
+    return;
   }
-  reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
-  reinterpret_cast<float4*>(Guide)[pixel] = make_float4(guide.x, guide.y, guide.z, 1.0f);
+  o.final = false;
+  int sample = cam.sample;
+  float r1 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 1823u), 991);
+  float r2 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 971u), 731);
+  f3 su = basisU(sun);
+  f3 sv = cross3(sun, su);
+  float angle = r1 * 6.28318f;
+  float disk = sqrtf(r2) * 0.012f;
+  f3 light = norm3(sun + su * (xcos(angle) * disk) + sv * (xsin(angle) * disk));
+  float offset = id >= 0 ? 0.0014f : 0.004f;
+  o.light = light;
+  o.origin = p + light * offset;
+  o.shadow = cam.shadows > 0.5f;
+  float nl = sat(dot3(n, light));
+  float back = sat(-dot3(n, light));
+  f3 direct = albedo * (nl / kPi);
+  if (leaf) {
+    float vein = leaf_vein(load_leaf(P, id, time + phase, wind), localP, localFp);
+    direct = direct + albedo * (back * (0.75f - 0.25f * vein) + xpow(sat(dot3(rd, light)), 9.0f) * 0.12f);
+  }
+  float spec = spec_ggx(n, rd * -1.0f, light, leaf ? 0.39f : 0.82f);
+  o.direct = direct + mk(spec, spec, spec);
+  float ao = 1.0f;
+  f3 ambient = mk(0.30f, 0.37f, 0.45f) * (0.45f + 0.55f * sat(n.y)) * ao + mk(0.08f, 0.068f, 0.035f) * sat(-n.y);
+  if (leaf) ambient = ambient + mk(0.04f, 0.055f, 0.022f) * ao;
+  o.ambientTerm = albedo * ambient;
+  o.haze = 1.0f - xexp(-t * 0.0018f);
+}
+__device__ __forceinline__ f3 shade_post(const Shading& o, f3 visibility) {
+  if (o.final) return o.debug;
+  f3 col = o.direct * visibility * mk(4.8f, 4.2f, 3.1f) + o.ambientTerm;
+  return mix3(col, o.skyc, o.haze);
+}
+
+// Shadow segments (Arbor.cu:271-274: at most four forest traces toward the
+// sun, 36 m, leaf transmission, any other hit opaque) run through the same
+// warp-batched tracer; a pixel without a shadow ray finishes when shaded.
+template <bool kForestScene>
+struct ShadePolicy {
+  const float* P;
+  float* Linear;
+  float* Guide;
+  const TraceCtx* ctx;
+  int pixel, seg;
+  f3 trans;
+  Shading sh;
+  __device__ __forceinline__ void write(f3 visibility) {
+    f3 col = shade_post(sh, visibility);
+    reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
+    reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);
+  }
+  __device__ __forceinline__ void done(Ray& r) {
+    int id = (int)r.found;
+    if (id < 0) {
+      write(trans);
+    } else if (ldg4(P, id * 6).w != 1.0f) {
+      write(mk(0.0f, 0.0f, 0.0f));
+    } else {
+      trans = trans * mk(0.18f, 0.29f, 0.065f);
+      sh.origin = sh.origin + sh.light * (r.best + 0.0018f);
+      if (++seg < 4) {
+        ray_begin(*ctx, r, sh.origin, sh.light, 36.0f);
+        return;
+      }
+      write(trans);
+    }
+    r.phase = kPhIdle;
+  }
+};
+
+template <bool kForestScene>
+__global__ void __launch_bounds__(kBlock, 2) shade_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                          const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                          const float* __restrict__ Hit, float* __restrict__ Linear,
+                                                          float* __restrict__ Guide, int width, int height) {
+  extern __shared__ float4 batch_smem[];
+  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForestScene ? kForest : 1];
+  block_setup(C, cam, inst, kForestScene);
+  const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
+  int x, y;
+  tile_pixel(threadIdx.x, x, y);
+  ShadePolicy<kForestScene> policy;
+  policy.P = P;
+  policy.Linear = Linear;
+  policy.Guide = Guide;
+  policy.ctx = &c;
+  policy.pixel = y * width + x;
+  Ray r;
+  r.phase = kPhIdle;
+  if (x < width && y < height) {
+    shade_pre<kForestScene>(P, cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + policy.pixel), x, y, width, height, policy.sh);
+    if (!policy.sh.final && policy.sh.shadow) {
+      policy.trans = mk(1.0f, 1.0f, 1.0f);
+      policy.seg = 0;
+      ray_begin(c, r, policy.sh.origin, policy.sh.light, 36.0f);
+    } else {
+      policy.write(mk(1.0f, 1.0f, 1.0f));
+    }
+  }
+  batch_run(c, r, b, policy);
 }
 
 // ------------------------------------------------------ filter / resolve --
@@ -420,10 +514,14 @@ int trace_entry(const char* name, bool forest, const float* P, const float* Node
                        {Hit, empty ? 0 : image_bytes(width, height), true, 16, "Hit"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
+  if (!batch_smem_ready(forest ? (const void*)trace_kernel<true> : (const void*)trace_kernel<false>)) {
+    set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
+    return ARBOR_ERR_CUDA;
+  }
   if (forest)
-    trace_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_kernel<true><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
   else
-    trace_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_kernel<false><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
   count_launch();
   return check_launch(name);
 }
@@ -438,10 +536,14 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
                        {Guide, img, true, 16, "Guide"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
+  if (!batch_smem_ready(forest ? (const void*)shade_kernel<true> : (const void*)shade_kernel<false>)) {
+    set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
+    return ARBOR_ERR_CUDA;
+  }
   if (forest)
-    shade_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+    shade_kernel<true><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
   else
-    shade_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+    shade_kernel<false><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
   count_launch();
   return check_launch(name);
 }

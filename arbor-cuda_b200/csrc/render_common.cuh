@@ -2,7 +2,7 @@
 // block prologue shared by the trace/shade kernels and the work-counting
 // kernel.
 #pragma once
-#include "arbor_scene.cuh"
+#include "warpbatch.cuh"
 
 namespace arbor {
 namespace {

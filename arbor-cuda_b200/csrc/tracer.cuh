@@ -1,0 +1,233 @@
+// tracer.cuh - forest ray state machine.
+//
+// One ray per lane, advanced through the phases of the reference's
+// traceForest/traceTree (Arbor.cu:220-251):
+//
+//   DDA   one forest cell: bounding-sphere test, tree entry, cell advance
+//   TREE  one BVH step: test both children of an accepted interior node,
+//         descend nearest-first, or pop a deferred sibling
+//   LEAF  the ray sits at an accepted leaf (a candidate primitive)
+//   TREE_END  the tree has no accepted node left (finish_tree folds it in)
+//   DONE  the ray's result is final
+//
+// Every step is the reference's step on the same values (same cells, same
+// nodes, nearest child first, same acceptance tests), so a ray driven through
+// these phases visits exactly what traceForest visits.
+#pragma once
+#include "arbor_scene.cuh"
+
+namespace arbor {
+
+enum RayPhase : int { kPhDDA = 0, kPhTree = 1, kPhLeaf = 2, kPhDone = 3, kPhIdle = 4, kPhBlocked = 5, kPhTreeEnd = 6 };
+
+struct Ray {
+  f3 ro, rd;        // world ray
+  float best;       // world-space nearest t so far
+  float found;      // primitive id of best (as the reference's float), -1
+  int foundTree;    // tree of best, -1
+  // forest DDA (Arbor.cu:241-248)
+  int ix, iz, sx, sz, step;
+  float tx, tz, dx, dz, exit;
+  // the tree being traversed, in its local frame (Arbor.cu:247)
+  int tree;
+  f3 lro, lrd, linv;
+  float lcone, lbest, ltime, lsc;
+  int lfound;
+  int node, depth;
+  uint32_t pending;
+  float spanx;
+  int phase;
+};
+
+struct TraceCtx {
+  const float* P;
+  const float* Nodes;
+  const uint32_t* Order;
+  const Instance* inst;   // forest instance table (shared memory)
+  float cone, time, wind;
+  bool refine;            // primary rays refine wood with the SDF march; shadow rays do not
+  bool forest;            // false: the single-tree scene (identity instance)
+};
+
+__device__ __forceinline__ void load_node(const TraceCtx& c, int n, float4& lo, float4& hi) {
+  lo = ldg4(c.Nodes, 2 * n);
+  hi = ldg4(c.Nodes, 2 * n + 1);
+}
+
+// Tree entry with the root test (Arbor.cu:221-223).  Returns true when the
+// root is accepted and traversal starts.
+__device__ __forceinline__ bool enter_tree(const TraceCtx& c, Ray& r) {
+  r.lfound = -1;
+  r.node = 1;
+  r.depth = 0;
+  r.pending = 0u;
+  float4 lo, hi;
+  load_node(c, 1, lo, hi);
+  return node_accept(lo, hi, r.lro, r.linv, r.lbest, r.spanx);
+}
+
+// After a cell's tree: next crossing, exit test, advance (Arbor.cu:248).
+__device__ __forceinline__ void dda_advance(Ray& r) {
+  float next = r.tx < r.tz ? r.tx : r.tz;
+  if (next > r.exit || next > r.best) {
+    r.phase = kPhDone;
+    return;
+  }
+  if (r.tx < r.tz) {
+    r.ix += r.sx;
+    r.tx += r.dx;
+  } else {
+    r.iz += r.sz;
+    r.tz += r.dz;
+  }
+  r.step++;
+  r.phase = kPhDDA;
+}
+
+// The tree is exhausted: fold its local result into the world result
+// (Arbor.cu:247 for the forest; traceTree's return for the single tree).
+__device__ __forceinline__ void finish_tree(const TraceCtx& c, Ray& r) {
+  if (!c.forest) {
+    r.best = r.lbest;
+    r.found = (float)r.lfound;
+    r.phase = kPhDone;
+    return;
+  }
+  if (r.lfound >= 0 && r.lbest * r.lsc < r.best) {
+    r.best = r.lbest * r.lsc;
+    r.found = (float)r.lfound;
+    r.foundTree = r.tree;
+  }
+  dda_advance(r);
+}
+
+// Begin a trace of (ro, rd) with initial nearest `best` (Arbor.cu:236-244).
+__device__ __forceinline__ void ray_begin(const TraceCtx& c, Ray& r, f3 ro, f3 rd, float best) {
+  r.ro = ro;
+  r.rd = rd;
+  r.best = best;
+  r.found = -1.0f;
+  r.foundTree = -1;
+  r.tree = -1;
+  if (!c.forest) {
+    r.lro = ro;
+    r.lrd = rd;
+    r.linv = inv3(rd);
+    r.lcone = c.cone;
+    r.lbest = best;
+    r.ltime = c.time;
+    r.lsc = 1.0f;
+    r.phase = enter_tree(c, r) ? kPhTree : kPhDone;
+    if (r.phase == kPhDone) finish_tree(c, r);
+    return;
+  }
+  const float half = (float)kSide * kSpacing * 0.5f;
+  f2 worldSpan = box_span(ro, rd, mk(-half, -1.2f, -half), mk(half, 13.5f, half));
+  float enter = fmaxf(0.0f, worldSpan.x);
+  r.exit = fminf(best, worldSpan.y);
+  if (r.exit < enter) {
+    r.phase = kPhDone;
+    return;
+  }
+  f3 pos = ro + rd * (enter + 0.0002f);
+  r.ix = (int)floorf(pos.x / kSpacing + (float)kSide * 0.5f + 0.5f);
+  r.iz = (int)floorf(pos.z / kSpacing + (float)kSide * 0.5f + 0.5f);
+  r.sx = rd.x >= 0.0f ? 1 : -1;
+  r.sz = rd.z >= 0.0f ? 1 : -1;
+  float invx = inv_safe(rd.x);
+  float invz = inv_safe(rd.z);
+  float bx = ((float)(r.ix - kSide / 2) + (r.sx > 0 ? 0.5f : -0.5f)) * kSpacing;
+  float bz = ((float)(r.iz - kSide / 2) + (r.sz > 0 ? 0.5f : -0.5f)) * kSpacing;
+  r.tx = (bx - ro.x) * invx;
+  r.tz = (bz - ro.z) * invz;
+  r.dx = kSpacing * fabsf(invx);
+  r.dz = kSpacing * fabsf(invz);
+  r.step = 0;
+  r.phase = kPhDDA;
+}
+
+// One forest cell (Arbor.cu:245-247).
+__device__ __forceinline__ void dda_step(const TraceCtx& c, Ray& r) {
+  if (r.step >= 48 || r.ix < 0 || r.iz < 0 || r.ix >= kSide || r.iz >= kSide) {
+    r.phase = kPhDone;
+    return;
+  }
+  int tree = r.iz * kSide + r.ix;
+  ARBOR_COUNT(kEvCell);
+  const Instance& it = c.inst[tree];
+  float broad = sphere_t(r.ro, r.rd, mk(it.px + 0.0f, 0.0f + it.cy, it.pz + 0.0f), it.rad);
+  if (broad < r.best) {
+    ARBOR_COUNT(kEvTree);
+    r.tree = tree;
+    r.lro = to_local_point(r.ro, it);
+    r.lrd = to_local_dir(r.rd, it);
+    r.linv = inv3(r.lrd);
+    r.lcone = c.cone / it.sc;
+    r.lbest = r.best / it.sc;
+    r.ltime = c.time + it.phase;
+    r.lsc = it.sc;
+    if (enter_tree(c, r)) {
+      r.phase = kPhTree;
+      return;
+    }
+    finish_tree(c, r);  // root rejected: traceTree returns (best, -1)
+    return;
+  }
+  dda_advance(r);
+}
+
+// Pop deferred siblings, deepest first, until one is still accepted
+// (the reference's stack pop and re-test, Arbor.cu:223, 227).
+__device__ __forceinline__ bool pop_next(const TraceCtx& c, Ray& r) {
+  while (r.pending != 0u) {
+    int level = 31 - __clz(r.pending);
+    r.pending &= ~(1u << level);
+    r.node = (r.node >> (r.depth - level)) ^ 1;
+    r.depth = level;
+    float4 lo, hi;
+    load_node(c, r.node, lo, hi);
+    if (node_accept(lo, hi, r.lro, r.linv, r.lbest, r.spanx)) return true;
+  }
+  return false;
+}
+
+// One interior step (Arbor.cu:224-225, 227).
+__device__ __forceinline__ void tree_step(const TraceCtx& c, Ray& r) {
+  if (r.node >= kCapacity) {
+    r.phase = kPhLeaf;
+    return;
+  }
+  int left = r.node * 2;
+  float4 llo, lhi, rlo, rhi;
+  load_node(c, left, llo, lhi);
+  load_node(c, left + 1, rlo, rhi);
+  float lx, rx;
+  bool lh = node_accept(llo, lhi, r.lro, r.linv, r.lbest, lx);
+  bool rh = node_accept(rlo, rhi, r.lro, r.linv, r.lbest, rx);
+  if (lh || rh) {
+    r.depth++;
+    if (lh && rh) {
+      bool l = lx < rx;
+      r.pending |= 1u << r.depth;
+      r.node = l ? left : left + 1;
+      r.spanx = l ? lx : rx;
+    } else if (lh) {
+      r.node = left;
+      r.spanx = lx;
+    } else {
+      r.node = left + 1;
+      r.spanx = rx;
+    }
+    if (r.node >= kCapacity) r.phase = kPhLeaf;
+    return;
+  }
+  if (pop_next(c, r)) {
+    r.phase = r.node >= kCapacity ? kPhLeaf : kPhTree;
+    return;
+  }
+  // The tree is exhausted.  The driver folds the tree's result in
+  // (finish_tree) once every test it queued for this tree has come back.
+  r.phase = kPhTreeEnd;
+}
+
+}  // namespace arbor

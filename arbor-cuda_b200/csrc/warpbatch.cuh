@@ -1,0 +1,229 @@
+// warpbatch.cuh - warp-batched primitive tests for forest rays.
+//
+// The reference tests one candidate primitive at a time inside its BVH loop
+// (Arbor.cu:226).  On a GPU that serialises a warp: the rare, long tests
+// (the leaf Newton solve, the bark SDF march) run with one or two lanes
+// active.  Here each lane traverses on its own (tracer.cuh) and, instead of
+// testing a candidate, queues it (up to kQueue per lane) and keeps
+// traversing; when every lane is blocked (queue full, tree finished, ray
+// done) the warp runs all queued tests as compacted jobs - leaf clips, then
+// Newton solves of the clips that pass, wood tests and the rest - one job per
+// lane, and each lane applies its results in candidate order.
+//
+// Why results do not change: every primitive surface lies inside the
+// primitive's own bounding box (the leaf-frame box, petiole, bark relief and
+// ellipsoid are all inside boundLow/boundHigh, Arbor.cu:132-133), so a hit t
+// is never below the box's entry span.x, and the reference only prunes boxes
+// with span.x >= best.  A primitive it prunes therefore cannot beat its final
+// answer, and the answer is the nearest hit over the accepted leaf boxes
+// whatever the order of the tests.  Traversing past a queued candidate with
+// the not-yet-updated best only adds tests that cannot win; the footprint of
+// each test depends only on its own box (Arbor.cu:226).  The one difference is
+// the order in which exactly equal t values are met.  The DDA advance and
+// tree hand-over wait for all results, so they use the reference's best.
+#pragma once
+#include "tracer.cuh"
+
+namespace arbor {
+
+constexpr int kQueue = 8;        // candidates a lane may queue
+constexpr int kWarpJobs = 32 * kQueue;
+constexpr int kNewtonCap = 64;   // pending Newton solves per warp
+
+struct WarpBatch {
+  float4 rayO[32];             // owner lane's local ray origin and wind time
+  float4 rayD[32];             // owner lane's local ray direction
+  LeafSolve solve[kNewtonCap];
+  int prim[kWarpJobs];         // lane-major queue: lane * kQueue + k
+  float fp[kWarpJobs];
+  int type[kWarpJobs];
+  float res[kWarpJobs];
+  short leafJob[kWarpJobs];    // compacted job lists (queue indices)
+  short woodJob[kWarpJobs];
+  short miscJob[kWarpJobs];
+  short solveJob[kNewtonCap];
+};
+
+// Advance one lane until its queue is full, its tree is finished with tests
+// pending, or its ray is done.
+__device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WarpBatch& b, int lane, int& nq) {
+  while (r.phase == kPhDDA || r.phase == kPhTree || r.phase == kPhLeaf || r.phase == kPhTreeEnd) {
+    if (r.phase == kPhDDA) {
+      dda_step(c, r);
+      continue;
+    }
+    if (r.phase == kPhTree) {
+      tree_step(c, r);
+      continue;
+    }
+    if (r.phase == kPhTreeEnd) {
+      if (nq > 0) return;  // the tree's queued tests must come back first
+      finish_tree(c, r);
+      continue;
+    }
+    // an accepted leaf: queue its primitive
+    uint32_t uid = __ldg(c.Order + (r.node - kCapacity));
+    if (uid < (uint32_t)kCapacity) {  // an Order entry past the records is skipped, not read
+      int q = lane * kQueue + nq++;
+      b.prim[q] = (int)uid;
+      b.fp[q] = fmaxf(0.000005f, r.lcone * fmaxf(0.05f, r.spanx));
+      b.type[q] = (int)ldg4(c.P, (int)uid * 6).w;
+      if (nq == kQueue) {
+        r.phase = kPhBlocked;  // resume with the pop once results are in
+        return;
+      }
+    }
+    if (pop_next(c, r)) {
+      r.phase = r.node >= kCapacity ? kPhLeaf : kPhTree;
+    } else if (nq > 0) {
+      r.phase = kPhTreeEnd;
+      return;
+    } else {
+      finish_tree(c, r);
+    }
+  }
+}
+
+// Run every queued test of the warp.  All 32 lanes call it together.
+__device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WarpBatch& b, int lane, int nq) {
+  const unsigned full = 0xffffffffu;
+  const unsigned lt = (1u << lane) - 1u;
+  if (nq > 0) {
+    b.rayO[lane] = make_float4(r.lro.x, r.lro.y, r.lro.z, r.ltime);
+    b.rayD[lane] = make_float4(r.lrd.x, r.lrd.y, r.lrd.z, 0.0f);
+  }
+  // per-lane counts by class, scanned across the warp
+  int nl = 0, nw = 0, nm = 0;
+  for (int k = 0; k < nq; k++) {
+    int t = b.type[lane * kQueue + k];
+    if (t == 1)
+      nl++;
+    else if (t == 0 && c.refine)
+      nw++;
+    else
+      nm++;
+  }
+  int sl = nl, sw = nw, sm = nm;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int a = __shfl_up_sync(full, sl, o), d = __shfl_up_sync(full, sw, o), e = __shfl_up_sync(full, sm, o);
+    if (lane >= o) {
+      sl += a;
+      sw += d;
+      sm += e;
+    }
+  }
+  const int totL = __shfl_sync(full, sl, 31), totW = __shfl_sync(full, sw, 31), totM = __shfl_sync(full, sm, 31);
+  int ol = sl - nl, ow = sw - nw, om = sm - nm;
+  for (int k = 0; k < nq; k++) {
+    int q = lane * kQueue + k;
+    int t = b.type[q];
+    if (t == 1)
+      b.leafJob[ol++] = (short)q;
+    else if (t == 0 && c.refine)
+      b.woodJob[ow++] = (short)q;
+    else
+      b.miscJob[om++] = (short)q;
+  }
+  __syncwarp();
+  // leaf clips; the clips that pass queue a Newton solve
+  int nN = 0;
+  for (int base = 0; base < totL; base += 32) {
+    int j = base + lane;
+    bool solve = false;
+    LeafSolve ls;
+    int q = 0;
+    if (j < totL) {
+      q = b.leafJob[j];
+      int owner = q / kQueue;
+      float4 o = b.rayO[owner], d = b.rayD[owner];
+      solve = leaf_clip(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls);
+      if (!solve) b.res[q] = ls.best;
+    }
+    unsigned m = __ballot_sync(full, solve);
+    if (solve) {
+      int pos = nN + __popc(m & lt);
+      b.solve[pos] = ls;
+      b.solveJob[pos] = (short)q;
+    }
+    nN += __popc(m);
+    __syncwarp();
+    if (nN >= 32) {  // a full pass of Newton solves
+      int qn = b.solveJob[lane];
+      b.res[qn] = leaf_newton(b.solve[lane], b.fp[qn]);
+      __syncwarp();
+      if (lane < nN - 32) {
+        b.solve[lane] = b.solve[32 + lane];
+        b.solveJob[lane] = b.solveJob[32 + lane];
+      }
+      nN -= 32;
+      __syncwarp();
+    }
+  }
+  if (lane < nN) {
+    int qn = b.solveJob[lane];
+    b.res[qn] = leaf_newton(b.solve[lane], b.fp[qn]);
+  }
+  // wood tests (tube + SDF march)
+  for (int base = 0; base < totW; base += 32) {
+    int j = base + lane;
+    if (j < totW) {
+      int q = b.woodJob[j];
+      int owner = q / kQueue;
+      float4 o = b.rayO[owner], d = b.rayD[owner];
+      b.res[q] = wood_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], true);
+    }
+  }
+  // stones, shadow-ray wood and unused records
+  for (int base = 0; base < totM; base += 32) {
+    int j = base + lane;
+    if (j < totM) {
+      int q = b.miscJob[j];
+      int owner = q / kQueue;
+      float4 o = b.rayO[owner], d = b.rayD[owner];
+      b.res[q] = object_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], o.w, c.wind, c.refine);
+    }
+  }
+  __syncwarp();
+}
+
+// Apply a lane's results in candidate order and resume it.
+__device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, const WarpBatch& b, int lane, int& nq) {
+  for (int k = 0; k < nq; k++) {
+    float t = b.res[lane * kQueue + k];
+    if (t < r.lbest) {
+      r.lbest = t;
+      r.lfound = b.prim[lane * kQueue + k];
+    }
+  }
+  nq = 0;
+  if (r.phase == kPhBlocked) {
+    if (pop_next(c, r))
+      r.phase = r.node >= kCapacity ? kPhLeaf : kPhTree;
+    else
+      finish_tree(c, r);
+  } else if (r.phase == kPhTreeEnd) {
+    finish_tree(c, r);
+  }
+}
+
+// Drive one warp's rays to completion.  Policy::done(r) is called for a
+// finished ray and either starts a new trace on r or sets it idle.
+template <class Policy>
+__device__ __forceinline__ void batch_run(const TraceCtx& c, Ray& r, WarpBatch& b, Policy& policy) {
+  const int lane = threadIdx.x & 31;
+  int nq = 0;
+  for (;;) {
+    for (;;) {
+      batch_advance(c, r, b, lane, nq);
+      if (r.phase != kPhDone) break;
+      policy.done(r);
+    }
+    const bool pending = nq > 0;
+    if (!__any_sync(0xffffffffu, pending)) break;  // every lane idle
+    batch_tests(c, r, b, lane, nq);
+    batch_apply(c, r, b, lane, nq);
+  }
+}
+
+}  // namespace arbor
