@@ -58,6 +58,7 @@ SIGNATURES = {
     "arbor_reduceBounds": (_i, [_vp, _i, _vp]),
     "arbor_initCamera": (_i, [_vp, _vp, _i, _vp]),
     "arbor_updateCamera": (_i, [_vp, _vp, _vp, _f, _i, _i, _vp]),
+    "arbor_setSample": (_i, [_vp, _i, _i, _vp]),
     "arbor_tracePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_shadePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_filterLighting": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),

@@ -107,10 +107,30 @@ __global__ void update_camera_kernel(float* C, const float* I, float delta, int 
   C[9] = C[10] > 0.5f ? 0.0f : fminf(255.0f, C[9] + 1.0f);
 }
 
+// Sample index and history reset for progressive sampling, as the harness
+// writes them before each sample (tests/native_harness.cpp:62).
+__global__ void set_sample_kernel(float* C, int sample, int reset) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  C[9] = (float)sample;
+  C[10] = reset ? 1.0f : 0.0f;
+}
+
 }  // namespace
 }  // namespace arbor
 
 using namespace arbor;
+
+extern "C" int arbor_setSample(float* C, int sample, int reset, arbor_stream stream) {
+  const Binding b[] = {{C, kC, true, 4, "C"}};
+  if (int s = check_bindings("arbor_setSample", b)) return s;
+  if (sample < 0 || sample > 16777216) {
+    set_error("arbor_setSample: sample %d outside 0..2^24 (C[9] is a float)", sample);
+    return ARBOR_ERR_VALUE;
+  }
+  set_sample_kernel<<<1, 1, 0, stream>>>(C, sample, reset);
+  count_launch();
+  return check_launch("arbor_setSample");
+}
 
 extern "C" int arbor_initCamera(float* C, const float* P, int seed, arbor_stream stream) {
   const Binding b[] = {{C, kC, true, 4, "C"}, {P, kP, false, 4, "P"}};

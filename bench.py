@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="arbor", choices=["arbor", "reference"])
-    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "tree"])
+    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "wind", "tree"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--width", type=int, default=0, help="override the workload's width (profiling runs)")
@@ -55,16 +55,20 @@ def parse():
 
 
 def workload_spec(name: str) -> dict:
+    base = {"seed": 7, "width": 1920, "height": 1080, "spp": 1, "shadows": False, "single_tree": False, "wind": False, "rebuild": False}
     if name == "forest":
-        return {"workload": "forest-1080p-walk: 324-tree forest from master seed 7, 1920x1080, 1 spp, sun shadows off, "
-                            "64-frame seeded walk at 1.4 m/s, eye height 1.72 m",
-                "seed": 7, "width": 1920, "height": 1080, "spp": 1, "shadows": False, "single_tree": False}
+        return {**base, "workload": "forest-1080p-walk: 324-tree forest from master seed 7, 1920x1080, 1 spp, sun shadows off, "
+                                    "64-frame seeded walk at 1.4 m/s, eye height 1.72 m"}
     if name == "shadows":
-        return {"workload": "forest-1080p-walk-shadows: the forest walk with tree-to-tree sun shadows on "
-                            "(sun elevation 35 deg, azimuth from the seed)",
-                "seed": 7, "width": 1920, "height": 1080, "spp": 1, "shadows": True, "single_tree": False}
-    return {"workload": "tree-256: one tree from master seed 1, 256x256, 1 spp, 6 m camera, 60 deg FOV, shadows off",
-            "seed": 1, "width": 256, "height": 256, "spp": 1, "shadows": False, "single_tree": True}
+        return {**base, "shadows": True,
+                "workload": "forest-1080p-walk-shadows: the forest walk with tree-to-tree sun shadows on "
+                            "(sun elevation 35 deg, azimuth from the seed)"}
+    if name == "wind":
+        return {**base, "shadows": True, "wind": True, "rebuild": True, "spp": 4,
+                "workload": "forest-1080p-wind: the forest walk at 4 spp per frame, sun shadows on (35 deg, azimuth from the seed), "
+                            "wind-animated leaves, scene and BVH rebuilt every frame"}
+    return {**base, "seed": 1, "width": 256, "height": 256, "single_tree": True,
+            "workload": "tree-256: one tree from master seed 1, 256x256, 1 spp, 6 m camera, 60 deg FOV, shadows off"}
 
 
 # ----------------------------------------------------------------- clocks --
@@ -153,11 +157,7 @@ class Frames:
         if spec["single_tree"]:
             self.C.copy_(torch.from_numpy(workloads.single_tree_camera(w, h, spec["seed"])))
         else:
-            c = self.C.cpu().numpy()
-            c[22] = 1.0 if spec["shadows"] else 0.0
-            if spec["shadows"]:
-                c[12], c[13] = workloads.shadow_sun(spec["seed"])
-            self.C.copy_(torch.from_numpy(c))
+            self.C.copy_(torch.from_numpy(workload_state(self.C.cpu().numpy(), spec)))
         inputs = np.zeros((WALK_FRAMES, 32), np.float32)
         self.dts = []
         for k in range(WALK_FRAMES):
@@ -172,14 +172,43 @@ class Frames:
         if st != self.ab.OK:
             raise RuntimeError(f"{self.ab.STATUS.get(st)}: {self.ab.last_error()}")
 
-    def step(self, k: int):
+    def build(self):
+        """The per-frame scene rebuild (camera record untouched)."""
+        self.check(self.ab.call("arbor_buildScene", self.spec["seed"], self.B, self.P, self.Keys, self.Order, self.Nodes, None, self.scratch))
+
+    def sample(self):
         ab, w, h = self.ab, self.w, self.h
-        if not self.spec["single_tree"]:
-            Ik = self.I[k % WALK_FRAMES]
-            self.check(ab.call("arbor_updateCamera", self.C, Ik, self.P, self.dts[k % WALK_FRAMES], w, h))
         self.check(ab.call(self.trace, self.P, self.Nodes, self.Order, self.C, self.Hit, w, h))
         self.check(ab.call(self.shade, self.P, self.Nodes, self.Order, self.C, self.Hit, self.Lin, self.Gui, w, h))
         self.check(ab.call("arbor_filterResolve", self.Lin, self.Gui, self.Hit, self.Fil, self.Hist, self.Pix, self.C, w, h))
+
+    def step(self, k: int):
+        ab, w, h = self.ab, self.w, self.h
+        if self.spec["rebuild"]:
+            self.build()
+        if not self.spec["single_tree"]:
+            Ik = self.I[k % WALK_FRAMES]
+            self.check(ab.call("arbor_updateCamera", self.C, Ik, self.P, self.dts[k % WALK_FRAMES], w, h))
+        spp = self.spec["spp"]
+        for s in range(spp):
+            if spp > 1:
+                # progressive samples of one frame, as the harness's render loop
+                # sets C[9] and C[10] (tests/native_harness.cpp:62)
+                self.check(ab.call("arbor_setSample", self.C, s, int(s == 0)))
+            self.sample()
+
+
+def workload_state(C: np.ndarray, spec: dict) -> np.ndarray:
+    """The camera/state record of a forest workload on top of initCamera's."""
+    import workloads
+
+    C = C.copy()
+    C[22] = 1.0 if spec["shadows"] else 0.0
+    if spec["shadows"]:
+        C[12], C[13] = workloads.shadow_sun(spec["seed"])
+    if spec.get("wind"):
+        C[11] = 0.60  # the breeze toggle's amplitude (Arbor.cu:182)
+    return C
 
 
 def time_kernel(torch, fn, reps: int) -> float:
@@ -249,6 +278,7 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
     ms_trace = time_kernel(torch, lambda: fr.check(ab.call(fr.trace, fr.P, fr.Nodes, fr.Order, fr.C, fr.Hit, w, h)), reps)
     ms_shade = time_kernel(torch, lambda: fr.check(ab.call(fr.shade, fr.P, fr.Nodes, fr.Order, fr.C, fr.Hit, fr.Lin, fr.Gui, w, h)), reps)
     ms_fr = time_kernel(torch, lambda: fr.check(ab.call("arbor_filterResolve", fr.Lin, fr.Gui, fr.Hit, fr.Fil, fr.Hist, fr.Pix, fr.C, w, h)), reps * 4)
+    ms_build = time_kernel(torch, fr.build, reps * 4)
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs")
     # filterLighting+resolvePixels algorithmic bytes per pixel: Linear, Guide,
@@ -267,7 +297,9 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
         "config": {**{k: v for k, v in spec.items()}, "frames_in_walk": WALK_FRAMES, "parallelism": f"replicas x{world}",
                    "l2": "per-step frame buffers (Hit, Linear, Guide, Filtered, History, Pixels = 174 MB at 1080p) exceed the "
                          "126 MB L2; the 5.7 MB scene stays resident by design"},
-        "phases_ms": {"trace": round(ms_trace, 4), "shade": round(ms_shade, 4), "filter_resolve": round(ms_fr, 4)},
+        "phases_ms": {"trace": round(ms_trace, 4), "shade": round(ms_shade, 4), "filter_resolve": round(ms_fr, 4),
+                      "build": round(ms_build, 4), "per_sample": ["trace", "shade", "filter_resolve"],
+                      "per_frame": (["build"] if spec["rebuild"] else []) + ["update_camera"] + (["set_sample"] if spec["spp"] > 1 else [])},
         "roofline": None,
         "roofline_hbm": {"kernel": "filterResolve", "bound": "hbm", "achieved": round(fr_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(fr_gbs / hbm_peak, 4) if hbm_peak else None, "traffic": None,
@@ -284,7 +316,10 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
 
     # End to end through the engine API with host buffers.
     if not args.no_e2e:
-        result["e2e"] = run_e2e(ab, torch, spec, args)
+        if spec["spp"] == 1 and not spec["rebuild"]:
+            result["e2e"] = run_e2e(ab, torch, spec, args)
+        else:
+            result["e2e"] = {"value": None, "unit": UNIT, "note": "the engine API renders one sample per frame without rebuilds"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(spec, args.cpu_seconds)
     if rank == 0:
@@ -304,9 +339,7 @@ def run_e2e(ab, torch, spec: dict, args) -> dict:
         if spec["single_tree"]:
             state = workloads.single_tree_camera(w, h, spec["seed"])
         else:
-            state[22] = 1.0 if spec["shadows"] else 0.0
-            if spec["shadows"]:
-                state[12], state[13] = workloads.shadow_sun(spec["seed"])
+            state = workload_state(state, spec)
         eng.set_state(state)
         host = torch.empty(w * h, dtype=torch.int32).pin_memory()
         n = w * h
@@ -360,10 +393,7 @@ class CpuFrame:
         if spec["single_tree"]:
             C = workloads.single_tree_camera(w, h, seed)
         else:
-            C = o.init_camera(self.scene["P"], seed)
-            C[22] = 1.0 if spec["shadows"] else 0.0
-            if spec["shadows"]:
-                C[12], C[13] = workloads.shadow_sun(seed)
+            C = workload_state(o.init_camera(self.scene["P"], seed), spec)
             I, dt = workloads.walk_input(0, seed)
             o.update_camera(C, I, self.scene["P"], dt, w, h)
         self.C = C
@@ -377,8 +407,12 @@ class CpuFrame:
 
     def render(self, n: int) -> tuple[int, float, int]:
         rows = self.rows(n)
+        spp = self.spec["spp"]
         t0 = time.perf_counter()
-        self.o.frame_rows(self.scene, self.C, self.spec["width"], self.spec["height"], rows, self.bufs, single=self.spec["single_tree"])
+        for s in range(spp):
+            if spp > 1:
+                self.C[9], self.C[10] = s, float(s == 0)
+            self.o.frame_rows(self.scene, self.C, self.spec["width"], self.spec["height"], rows, self.bufs, single=self.spec["single_tree"])
         secs = time.perf_counter() - t0
         return len(rows) * self.spec["width"] * self.spec["spp"], secs, len(rows)
 

@@ -127,6 +127,11 @@ ARBOR_API int arbor_initCamera(float* C, const float* P, int seed, arbor_stream 
  * scalars delta (finite), width, height). */
 ARBOR_API int arbor_updateCamera(float* C, const float* I, const float* P, float delta, int width, int height, arbor_stream stream);
 
+/* Progressive sampling control (no reference kernel; the harness writes these
+ * fields directly before each sample, tests/native_harness.cpp:62):
+ * C[9] = sample, C[10] = reset ? 1 : 0.  sample must lie in 0..2^24. */
+ARBOR_API int arbor_setSample(float* C, int sample, int reset, arbor_stream stream);
+
 /* Primary hit per pixel: Hit[4*px] = {t, primId, treeId, footprint}
  * (Arbor.cu:252; bindings P, Nodes, Order, C r; Hit w; scalars width, height). */
 ARBOR_API int arbor_tracePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height, arbor_stream stream);
