@@ -1,0 +1,469 @@
+// passes.cuh - per-tile device code of the image passes, shared by the
+// single-image kernels (render.cu) and the batched renderer (batch.cu):
+// the trace and shade of one tile of pixels, the shading functions
+// (Arbor.cu:256-289) and the filter / resolve of one tile (Arbor.cu:292-304).
+#pragma once
+#include "render_common.cuh"
+
+namespace arbor {
+namespace {
+
+// A CTA's 256 threads cover a tile of tw x (256 / tw) pixels (tw = 16 or 32)
+// made of 8x4-pixel warps.
+__device__ __forceinline__ void tile_pixel_at(int t, int x0, int y0, int tw, int& x, int& y) {
+  int warp = t >> 5, lane = t & 31, across = tw >> 3;
+  x = x0 + (warp % across) * 8 + (lane & 7);
+  y = y0 + (warp / across) * 4 + (lane >> 3);
+}
+
+// ---------------------------------------------------------------- trace --
+// One ray per thread over 16x16-pixel CTAs (8x4-pixel warps); each warp's
+// primitive tests run warp-batched (warpbatch.cuh).
+struct PrimaryPolicy {
+  const Camera* cam;
+  float* Hit;
+  int width, height, pixel;
+  __device__ __forceinline__ void done(Ray& r) {
+    reinterpret_cast<float4*>(Hit)[pixel] = make_float4(r.best, r.found, (float)r.foundTree, cam->c14 * r.best / (float)height);
+    r.phase = kPhIdle;
+  }
+};
+
+// Primary rays of one tile (tracePixels, Arbor.cu:252).
+__device__ __forceinline__ void trace_tile(const TraceCtx& c, const Camera& cam, WarpBatch& b, float* __restrict__ Hit, int width, int height,
+                                           int x0, int y0, int tw) {
+  int x, y;
+  tile_pixel_at(threadIdx.x, x0, y0, tw, x, y);
+  PrimaryPolicy policy{&cam, Hit, width, height, y * width + x};
+  Ray r;
+  r.phase = kPhIdle;
+  if (x < width && y < height) {
+    f3 rd = camera_ray(cam, x, y, width, height);
+    float ground = rd.y < -0.00001f ? -cam.ro.y / rd.y : kFar;  // Arbor.cu:252
+    ray_begin(c, r, cam.ro, rd, ground > 0.0f ? ground : kFar);
+  }
+  batch_run(c, r, b, policy);
+}
+
+// ---------------------------------------------------------------- shade --
+// Arbor.cu:256
+__device__ f3 sky(f3 rd, f3 sun) {
+  float h = sat(rd.y);
+  f3 c = mix3(mk(0.75f, 0.79f, 0.77f), mk(0.19f, 0.35f, 0.54f), xpow(h, 0.48f));
+  float warm = xpow(sat(dot3(rd, sun)), 32.0f);
+  c = c + mk(0.48f, 0.26f, 0.075f) * warm;
+  float disc = smooth(0.99996f, 0.999984f, dot3(rd, sun));
+  c = c + mk(8.0f, 6.7f, 4.9f) * disc;
+  float clouds = noise(rd.x * 5.0f / (0.2f + h), rd.z * 5.0f / (0.2f + h), 231);
+  float veil = smooth(0.62f, 0.81f, clouds) * smooth(0.02f, 0.18f, h) * 0.38f;
+  return mix3(c, mk(1.1f, 1.10f, 1.05f), veil);
+}
+// Arbor.cu:257-263
+__device__ f3 bark_color(const float* P, int id, f3 p, float footprint) {
+  Wood w = load_wood(P, id);
+  f3 q = p - w.a;
+  float z = dot3(q, w.d);
+  float theta = atan2f(dot3(q, w.v), dot3(q, w.u));
+  float arc = w.arc0 + z;
+  f3 coord = mk(cosf(theta) * 9.0f, sinf(theta) * 9.0f, arc * 7.0f);
+  float mottle = noise3(p * 3.0f, 714);
+  float rough = noise3(coord, w.seed);
+  float t = sat(dot3(p - w.a, w.ab) / fmaxf(0.000001f, w.abab));
+  float amp = fminf(0.021f, lerpf(w.ra, w.rb, t) * 0.055f);
+  float cut = bark_cut(w, p, footprint, band_weight(0.010f, footprint), band_weight(0.0025f, footprint)) / fmaxf(0.00001f, amp);
+  f3 c = mix3(mk(0.10f, 0.075f, 0.050f), mk(0.25f, 0.21f, 0.16f), 0.25f + rough * 0.62f);
+  c = c * (0.75f + 0.35f * mottle);
+  c = c * (1.0f - 0.62f * smooth(0.28f, 0.85f, cut));
+  float moss = smooth(0.52f, 0.72f, noise3(p * 5.0f, 189)) * (1.0f - smooth(0.15f, 1.4f, p.y));
+  c = mix3(c, mk(0.045f, 0.064f, 0.018f), moss * 0.62f);
+  float lichen = smooth(0.65f, 0.77f, noise3(p * 23.0f, 27)) * smooth(0.25f, 0.65f, noise3(p * 90.0f, 712)) * band_weight(0.018f, footprint);
+  c = mix3(c, mk(0.31f, 0.33f, 0.23f), lichen * 0.5f);
+  float grain = (noise3(coord * 15.0f, w.seed) - 0.5f) * band_weight(0.0025f, footprint);
+  return c * (1.0f + grain * 0.38f);
+}
+// Arbor.cu:264
+__device__ float leaf_vein(const Leaf& l, f3 p, float footprint) {
+  f3 q = p - l.origin;
+  float x = dot3(q, l.u) - l.stem;
+  float y = dot3(q, l.v);
+  float len = l.len;
+  float mid = xexp(-fabsf(y) / fmaxf(0.00065f, footprint * 0.55f));
+  float fy = fracf((x - fabsf(y) * 0.70f) / len * 7.0f);
+  float dd = fminf(fy, 1.0f - fy) * len / 7.0f;
+  float lateral = xexp(-dd / fmaxf(0.00033f, footprint * 0.5f));
+  return sat(mid * 0.82f + lateral * 0.48f) * band_weight(0.003f, footprint);
+}
+// Arbor.cu:265-268
+__device__ f3 leaf_color(const Leaf& l, f3 p, float fp) {
+  float h = rnd(l.seed, 887);
+  f3 q = p - l.origin;
+  float x = dot3(q, l.u) - l.stem;
+  if (x < 0.0f) return mk(0.17f, 0.15f, 0.048f);
+  float y = dot3(q, l.v);
+  float v = leaf_vein(l, p, fp);
+  f3 c = mix3(mk(0.035f, 0.11f, 0.008f), mk(0.15f, 0.255f, 0.025f), h);
+  c = mix3(c, mk(0.22f, 0.26f, 0.055f), v * 0.57f);
+  float speck = (noise(x * 700.0f, y * 700.0f, l.seed) - 0.5f) * band_weight(0.0017f, fp);
+  float edge = smooth(0.78f, 1.0f, fabsf(y) / fmaxf(0.001f, leaf_width(x, l.len, l.width, band_weight(0.002f, fp))));
+  c = c * (1.0f + speck * 0.27f);
+  c = mix3(c, mk(0.23f, 0.20f, 0.05f), edge * 0.22f);
+  return c;
+}
+// Arbor.cu:269
+__device__ f3 ground_color(f3 p, float fp) {
+  float a = noise(p.x * 3.0f, p.z * 3.0f, 819);
+  float b = noise(p.x * 15.0f, p.z * 15.0f, 28);
+  float r = sqrtf(p.x * p.x + p.z * p.z);
+  float soil = 1.0f - smooth(4.1f, 6.8f, r + noise(p.x, p.z, 13));
+  f3 grass = mix3(mk(0.085f, 0.115f, 0.035f), mk(0.23f, 0.24f, 0.092f), a);
+  f3 dirt = mix3(mk(0.075f, 0.055f, 0.035f), mk(0.16f, 0.13f, 0.080f), b);
+  float moss = smooth(0.53f, 0.73f, a);
+  dirt = mix3(dirt, mk(0.049f, 0.079f, 0.022f), moss * 0.72f);
+  float grit = (noise(p.x * 200.0f, p.z * 200.0f, 127) - 0.5f) * band_weight(0.007f, fp);
+  return mix3(grass, dirt, soil) * (1.0f + grit * 0.40f);
+}
+// Arbor.cu:231-234
+__device__ f3 object_normal(const float* P, int id, f3 p, float fp, float time, float wind) {
+  int type = (int)ldg4(P, id * 6).w;
+  if (type == 0) {
+    Wood w = load_wood(P, id);
+    float fine = band_weight(0.010f, fp), grain = band_weight(0.0025f, fp);
+    float e = fmaxf(0.000035f, fminf(0.0005f, fp * 0.18f));
+    f3 dx = mk(e, 0.0f, 0.0f), dy = mk(0.0f, e, 0.0f), dz = mk(0.0f, 0.0f, e);
+    return norm3(mk(wood_field(w, p + dx, fp, fine, grain) - wood_field(w, p - dx, fp, fine, grain),
+                    wood_field(w, p + dy, fp, fine, grain) - wood_field(w, p - dy, fp, fine, grain),
+                    wood_field(w, p + dz, fp, fine, grain) - wood_field(w, p - dz, fp, fine, grain)));
+  }
+  if (type == 1) {
+    Leaf l = load_leaf(P, id, time, wind);
+    f3 q = p - l.origin;
+    float x = dot3(q, l.u) - l.stem;
+    float y = dot3(q, l.v);
+    if (x < 0.0f) {
+      f3 centre = l.origin + l.u * (x + l.stem);
+      return norm3(p - centre);
+    }
+    const float e = 0.0002f;
+    float hw2 = l.width * l.width, bw = band_weight(0.007f, fp);
+    float a = (leaf_height(x + e, y, l.len, hw2, l.curl, l.twist, bw) - leaf_height(x - e, y, l.len, hw2, l.curl, l.twist, bw)) / (2.0f * e);
+    float c = (leaf_height(x, y + e, l.len, hw2, l.curl, l.twist, bw) - leaf_height(x, y - e, l.len, hw2, l.curl, l.twist, bw)) / (2.0f * e);
+    return norm3(l.n - l.u * a - l.v * c);
+  }
+  f3 q = p - xyz(ldg4(P, id * 6));
+  f3 h = xyz(ldg4(P, id * 6 + 1));
+  return norm3(mk(q.x / (h.x * h.x), q.y / (h.y * h.y), q.z / (h.z * h.z)));
+}
+// Arbor.cu:270
+__device__ f3 surface_color(const float* P, int id, f3 p, float fp, float time, float wind) {
+  if (id < 0) return ground_color(p, fp);
+  float4 r0 = ldg4(P, id * 6);
+  int type = (int)r0.w;
+  if (type == 0) return bark_color(P, id, p, fp);
+  if (type == 1) return leaf_color(load_leaf(P, id, time, wind), p, fp);
+  float f = noise3(p * 42.0f, (int)ldg4(P, id * 6 + 3).w);
+  return mix3(mk(0.09f, 0.10f, 0.086f), mk(0.31f, 0.30f, 0.24f), f);
+}
+// Arbor.cu:276
+__device__ float spec_ggx(f3 n, f3 v, f3 l, float rough) {
+  f3 h = norm3(v + l);
+  float nh = sat(dot3(n, h));
+  float nv = fmaxf(0.002f, sat(dot3(n, v)));
+  float nl = sat(dot3(n, l));
+  float vh = sat(dot3(v, h));
+  float a = rough * rough;
+  float aa = a * a;
+  float den = nh * nh * (aa - 1.0f) + 1.0f;
+  float D = aa / (kPi * den * den);
+  float k = (rough + 1.0f) * (rough + 1.0f) * 0.125f;
+  float G = nv / (nv * (1.0f - k) + k) * nl / (nl * (1.0f - k) + k);
+  float F = 0.035f + 0.965f * xpow(1.0f - vh, 5.0f);
+  return D * G * F / (4.0f * nv + 0.0001f);
+}
+
+// shadePixels (Arbor.cu:277-289) is split at the sun-visibility call:
+// shade_pre computes everything before it, the shadow segments are traced by
+// the warp tracer, shade_post composes the colour.  Each value is computed
+// with the reference's operations in the reference's order; the colour
+// before haze is (direct * visibility) * (4.8, 4.2, 3.1) + albedo * ambient.
+struct Shading {
+  f3 direct, ambientTerm, skyc, guide, origin, light, debug;
+  float haze;
+  bool final;   // colour is `debug` (sky pixel or debug view mode): no visibility needed
+  bool shadow;  // visibility must be traced
+};
+
+// The single-tree scene uses the identity instance: tree-local point and
+// normal, phase 0, no tint.
+template <bool kForestScene>
+__device__ __noinline__ void shade_pre(const float* P, const Camera& cam, const Instance* inst, float4 hit, int x, int y, int width, int height,
+                          Shading& o) {
+  int pixel = y * width + x;
+  float t = hit.x;
+  int id = (int)hit.y;
+  int tree = (int)hit.z;
+  // IDs past the record / instance ranges cannot come from tracePixels; such
+  // input is shaded as ground rather than read out of bounds.
+  if (id >= kCapacity) id = -1;
+  if (tree >= kForest) tree = -1;
+  f3 ro = cam.ro;
+  f3 rd = camera_ray(cam, x, y, width, height);
+  f3 sun = cam.sun;
+  o.skyc = sky(rd, sun);
+  o.guide = mk(1.0f, 1.0f, 1.0f);
+  o.shadow = false;
+  if (!(t < kFar)) {
+    o.final = true;
+    o.debug = o.skyc;
+    return;
+  }
+  f3 p = ro + rd * t;
+  float fp = fmaxf(0.000005f, hit.w);
+  f3 localP = p;
+  f3 n = mk(0.0f, 1.0f, 0.0f);
+  float localFp = fp;
+  float phase = 0.0f;
+  const float time = cam.time, wind = cam.wind;
+  if (kForestScene) {
+    if (id >= 0 && tree >= 0) {
+      const Instance& it = inst[tree];
+      localP = to_local_point(p, it);
+      localFp = fp / it.sc;
+      phase = it.phase;
+      n = to_world_normal(object_normal(P, id, localP, localFp, time + phase, wind), it);
+    }
+  } else if (id >= 0) {
+    n = object_normal(P, id, localP, localFp, time, wind);
+  }
+  bool leaf = id >= 0 && ldg4(P, id * 6).w == 1.0f;
+  if (dot3(n, rd) > 0.0f) n = n * -1.0f;
+  if (id < 0) {
+    float e = fmaxf(0.001f, fp);
+    uint32_t h133 = hashU(133u);
+    float nx = (noise_h((p.x + e) * 18.0f, p.z * 18.0f, h133) - noise_h((p.x - e) * 18.0f, p.z * 18.0f, h133)) * 0.18f;
+    float nz = (noise_h(p.x * 18.0f, (p.z + e) * 18.0f, h133) - noise_h(p.x * 18.0f, (p.z - e) * 18.0f, h133)) * 0.18f;
+    n = norm3(mk(nx, 1.0f, nz));
+  }
+  f3 albedo = surface_color(P, id, id >= 0 ? localP : p, localFp, time + phase, wind);
+  if (kForestScene && tree >= 0) {
+    int ts = inst[tree].seed;
+    float hue = rnd(8, ts);
+    float age = rnd(9, ts);
+    float season = rnd(10, ts);
+    float dark = 0.76f + age * 0.38f;
+    f3 tint = mk(0.88f + 0.22f * hue, 0.84f + 0.28f * (1.0f - fabsf(hue - 0.55f)), 0.72f + 0.25f * (1.0f - hue));
+    if (leaf)
+      tint = mix3(tint, mk(1.12f, 0.88f, 0.48f), smooth(0.78f, 0.98f, season) * 0.38f);
+    else
+      tint = mix3(tint, mk(0.78f, 0.66f, 0.53f), season * 0.18f);
+    albedo = albedo * tint * dark;
+  }
+  o.guide = albedo;
+  if (cam.mode == 1.0f || cam.mode == 2.0f || cam.mode == 3.0f) {
+    // Debug views replace the colour whatever the lighting (Arbor.cu:286).
+    o.final = true;
+    if (cam.mode == 1.0f) {
+      float w0 = band_weight(0.065f, localFp);
+      float w1 = band_weight(0.005f, localFp);
+      float w2 = band_weight(0.001f, localFp);
+      o.debug = mk(w0 * 0.80f, w1 * 0.85f, w2 * 0.9f);
+    } else if (cam.mode == 2.0f) {
+      float hh = rnd(id + 177 + (tree + 1) * 71, 32);
+      o.debug = id < 0 ? mk(0.10f, 0.10f, 0.10f) : (leaf ? mk(0.1f, 0.3f + hh * 0.5f, 0.17f) : mk(0.47f + hh * 0.3f, 0.25f, 0.10f));
+    } else {
+      o.debug = n * 0.5f + mk(0.5f, 0.5f, 0.5f);
+    }
+    return;
+  }
+  o.final = false;
+  int sample = cam.sample;
+  float r1 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 1823u), 991);
+  float r2 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 971u), 731);
+  f3 su = basisU(sun);
+  f3 sv = cross3(sun, su);
+  float angle = r1 * 6.28318f;
+  float disk = sqrtf(r2) * 0.012f;
+  f3 light = norm3(sun + su * (xcos(angle) * disk) + sv * (xsin(angle) * disk));
+  float offset = id >= 0 ? 0.0014f : 0.004f;
+  o.light = light;
+  o.origin = p + light * offset;
+  o.shadow = cam.shadows > 0.5f;
+  float nl = sat(dot3(n, light));
+  float back = sat(-dot3(n, light));
+  f3 direct = albedo * (nl / kPi);
+  if (leaf) {
+    float vein = leaf_vein(load_leaf(P, id, time + phase, wind), localP, localFp);
+    direct = direct + albedo * (back * (0.75f - 0.25f * vein) + xpow(sat(dot3(rd, light)), 9.0f) * 0.12f);
+  }
+  float spec = spec_ggx(n, rd * -1.0f, light, leaf ? 0.39f : 0.82f);
+  o.direct = direct + mk(spec, spec, spec);
+  float ao = 1.0f;
+  f3 ambient = mk(0.30f, 0.37f, 0.45f) * (0.45f + 0.55f * sat(n.y)) * ao + mk(0.08f, 0.068f, 0.035f) * sat(-n.y);
+  if (leaf) ambient = ambient + mk(0.04f, 0.055f, 0.022f) * ao;
+  o.ambientTerm = albedo * ambient;
+  o.haze = 1.0f - xexp(-t * 0.0018f);
+}
+__device__ __forceinline__ f3 shade_post(const Shading& o, f3 visibility) {
+  if (o.final) return o.debug;
+  f3 col = o.direct * visibility * mk(4.8f, 4.2f, 3.1f) + o.ambientTerm;
+  return mix3(col, o.skyc, o.haze);
+}
+
+// Shadow segments (Arbor.cu:271-274: at most four forest traces toward the
+// sun, 36 m, leaf transmission, any other hit opaque) run through the same
+// warp-batched tracer; a pixel without a shadow ray finishes when shaded.
+template <bool kForestScene>
+struct ShadePolicy {
+  const float* P;
+  float* Linear;
+  float* Guide;
+  const TraceCtx* ctx;
+  int pixel, seg;
+  f3 trans;
+  Shading sh;
+  __device__ __forceinline__ void write(f3 visibility) {
+    f3 col = shade_post(sh, visibility);
+    reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
+    reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);
+  }
+  __device__ __forceinline__ void done(Ray& r) {
+    int id = (int)r.found;
+    if (id < 0) {
+      write(trans);
+    } else if (ldg4(P, id * 6).w != 1.0f) {
+      write(mk(0.0f, 0.0f, 0.0f));
+    } else {
+      trans = trans * mk(0.18f, 0.29f, 0.065f);
+      sh.origin = sh.origin + sh.light * (r.best + 0.0018f);
+      if (++seg < 4) {
+        ray_begin(*ctx, r, sh.origin, sh.light, 36.0f);
+        return;
+      }
+      write(trans);
+    }
+    r.phase = kPhIdle;
+  }
+};
+
+// One tile of shadePixels (Arbor.cu:277-289); c is the shadow-ray context.
+template <bool kForestScene>
+__device__ __forceinline__ void shade_tile(const TraceCtx& c, const Camera& cam, const Instance* inst, WarpBatch& b, const float* __restrict__ P,
+                                           const float* __restrict__ Hit, float* __restrict__ Linear, float* __restrict__ Guide, int width,
+                                           int height, int x0, int y0, int tw) {
+  int x, y;
+  tile_pixel_at(threadIdx.x, x0, y0, tw, x, y);
+  ShadePolicy<kForestScene> policy;
+  policy.P = P;
+  policy.Linear = Linear;
+  policy.Guide = Guide;
+  policy.ctx = &c;
+  policy.pixel = y * width + x;
+  Ray r;
+  r.phase = kPhIdle;
+  if (x < width && y < height) {
+    shade_pre<kForestScene>(P, cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + policy.pixel), x, y, width, height, policy.sh);
+    if (!policy.sh.final && policy.sh.shadow) {
+      policy.trans = mk(1.0f, 1.0f, 1.0f);
+      policy.seg = 0;
+      ray_begin(c, r, policy.sh.origin, policy.sh.light, 36.0f);
+    } else {
+      policy.write(mk(1.0f, 1.0f, 1.0f));
+    }
+  }
+  batch_run(c, r, b, policy);
+}
+
+// ------------------------------------------------------ filter / resolve --
+constexpr int kFX = 32, kFY = 8, kHalo = 2;
+constexpr int kSX = kFX + 2 * kHalo, kSY = kFY + 2 * kHalo;
+
+// Arbor.cu:303
+__device__ __forceinline__ float aces(float x) { return sat((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f)); }
+
+// Arbor.cu:304, one pixel.
+__device__ __forceinline__ void resolve_px(f3 current, float* __restrict__ History, uint32_t* __restrict__ Pixels, float c9, float c10,
+                                           float exposure, int x, int y, int width, int height) {
+  int i = y * width + x;
+  float count = c10 > 0.5f ? 0.0f : c9;
+  f3 mean = current;
+  if (!(count < 0.5f)) mean = mix3(xyz(reinterpret_cast<const float4*>(History)[i]), current, 1.0f / (count + 1.0f));
+  reinterpret_cast<float4*>(History)[i] = make_float4(mean.x, mean.y, mean.z, count + 1.0f);
+  f3 col = mean * exposure;
+  col = mk(aces(col.x), aces(col.y), aces(col.z));
+  col = mk(xpow(col.x, 1.0f / 2.2f), xpow(col.y, 1.0f / 2.2f), xpow(col.z, 1.0f / 2.2f));
+  float u = ((float)x / (float)width - 0.5f) * 2.0f;
+  float v = ((float)y / (float)height - 0.5f) * 2.0f;
+  col = col * (1.0f - 0.09f * (u * u + v * v));
+  Pixels[i] = pack_rgb(col);
+}
+
+// Same-surface 5x5 demodulated filter (Arbor.cu:292-302) of one 32x8 tile,
+// staged with a 2-pixel halo in shared memory so each input pixel is read
+// from HBM once per tile.  kResolve fuses resolvePixels on the filtered value.
+// Threads are laid out 32 x 8 (threadIdx.x, threadIdx.y).
+struct FilterTile {
+  float4 hit[kSY][kSX];
+  float3 lin[kSY][kSX];
+  float3 gui[kSY][kSX];
+  float w[5];
+};
+template <bool kResolve>
+__device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restrict__ Linear, const float* __restrict__ Guide,
+                                            const float* __restrict__ Hit, float* __restrict__ Filtered, float* __restrict__ History,
+                                            uint32_t* __restrict__ Pixels, float c9, float c10, float c15, float c20, int width, int height,
+                                            int x0, int y0) {
+  const int tid = threadIdx.y * kFX + threadIdx.x;
+  // Filter weights expf(-(j*j+k*k)*0.30f) for the 5 distinct radii 1,2,4,5,8.
+  if (tid < 5) {
+    const int r2[5] = {1, 2, 4, 5, 8};
+    s.w[tid] = xexp(-(float)r2[tid] * 0.30f);
+  }
+  const int hx0 = x0 - kHalo, hy0 = y0 - kHalo;
+  for (int k = tid; k < kSX * kSY; k += kFX * kFY) {
+    int sy = k / kSX, sx = k - sy * kSX;
+    int gx = hx0 + sx, gy = hy0 + sy;
+    if (gx >= 0 && gy >= 0 && gx < width && gy < height) {
+      int q = gy * width + gx;
+      s.hit[sy][sx] = __ldg(reinterpret_cast<const float4*>(Hit) + q);
+      float4 l = __ldg(reinterpret_cast<const float4*>(Linear) + q);
+      float4 g = __ldg(reinterpret_cast<const float4*>(Guide) + q);
+      s.lin[sy][sx] = make_float3(l.x, l.y, l.z);
+      s.gui[sy][sx] = make_float3(g.x, g.y, g.z);
+    }
+  }
+  __syncthreads();
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x < width && y < height) {
+    const int cx = threadIdx.x + kHalo, cy = threadIdx.y + kHalo;
+    float4 hb = s.hit[cy][cx];
+    float3 lc = s.lin[cy][cx], gc = s.gui[cy][cx];
+    f3 col = mk(lc.x, lc.y, lc.z);
+    f3 base = mk(gc.x, gc.y, gc.z) + mk(0.02f, 0.02f, 0.02f);
+    f3 sum = mk(0.0f, 0.0f, 0.0f);
+    float weight = 0.0f;
+    int id = (int)hb.y;
+    float depth = hb.x;
+    if (depth < kFar && c15 < 0.5f) {
+      int treeB = (int)hb.z;
+      float tol = fmaxf(0.005f, hb.w * 6.0f);
+      for (int j = -2; j <= 2; j++)
+        for (int k = -2; k <= 2; k++) {
+          int xx = x + k, yy = y + j;
+          if (xx < 0 || yy < 0 || xx >= width || yy >= height) continue;
+          float4 hq = s.hit[cy + j][cx + k];
+          if ((int)hq.y != id || (int)hq.z != treeB || fabsf(hq.x - depth) > tol) continue;
+          int r2 = j * j + k * k;
+          float w = r2 == 0 ? 1.0f : s.w[r2 == 1 ? 0 : r2 == 2 ? 1 : r2 == 4 ? 2 : r2 == 5 ? 3 : 4];
+          float3 c = s.lin[cy + j][cx + k], g3 = s.gui[cy + j][cx + k];
+          f3 g = mk(g3.x, g3.y, g3.z) + mk(0.02f, 0.02f, 0.02f);
+          sum = sum + mk(c.x / g.x, c.y / g.y, c.z / g.z) * w;
+          weight += w;
+        }
+      if (weight > 0.0f) col = mix3(col, (sum / weight) * base, 0.86f);
+    }
+    reinterpret_cast<float4*>(Filtered)[y * width + x] = make_float4(col.x, col.y, col.z, 1.0f);
+    if (kResolve) resolve_px(col, History, Pixels, c9, c10, c20, x, y, width, height);
+  }
+}
+
+}  // namespace
+}  // namespace arbor
