@@ -45,6 +45,25 @@ class EngineInfo(ctypes.Structure):
     ]
 
 
+class BatchView(ctypes.Structure):
+    _fields_ = [("scene", _i), ("width", _i), ("height", _i), ("reserved", _i), ("C", _f * 64)]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("tile_width", _i), ("ctas_per_sm", _i), ("order", _i), ("queue", _i)]
+
+    def as_dict(self) -> dict:
+        return {"tile_width": self.tile_width, "ctas_per_sm": self.ctas_per_sm, "order": self.order, "queue": self.queue}
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_scenes", _i), ("n_views", _i), ("total_pixels", ctypes.c_uint64), ("allocated_bytes", ctypes.c_uint64),
+        ("trace_tiles", _i), ("filter_tiles", _i), ("renders", ctypes.c_uint64), ("launches_per_render", ctypes.c_uint32),
+        ("config", BatchConfig),
+    ]
+
+
 SIGNATURES = {
     "arbor_last_error": (ctypes.c_char_p, []),
     "arbor_status_name": (ctypes.c_char_p, [_i]),
@@ -73,6 +92,7 @@ SIGNATURES = {
     "arbor_filterResolve": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_trace_work_slots": (ctypes.c_size_t, [_i, _i]),
     "arbor_traceWork": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
+    "arbor_shadeWork": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
     "arbor_engine_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, _i, _vp]),
     "arbor_engine_generate": (_i, [_vp, _i]),
     "arbor_engine_resize": (_i, [_vp, _i, _i]),
@@ -85,6 +105,17 @@ SIGNATURES = {
     "arbor_engine_read_pixels": (_i, [_vp, _vp, ctypes.c_size_t]),
     "arbor_engine_dispose": (_i, [_vp]),
     "arbor_engine_destroy": (_i, [_vp]),
+    "arbor_batch_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(_i), _i, ctypes.POINTER(BatchView), _i, _vp]),
+    "arbor_batch_set_cameras": (_i, [_vp, ctypes.POINTER(_f), _i]),
+    "arbor_batch_configure": (_i, [_vp, ctypes.POINTER(BatchConfig)]),
+    "arbor_batch_get_config": (_i, [_vp, ctypes.POINTER(BatchConfig)]),
+    "arbor_batch_autotune": (_i, [_vp, _i, ctypes.POINTER(BatchConfig), ctypes.POINTER(_f)]),
+    "arbor_batch_render": (_i, [_vp]),
+    "arbor_batch_profile": (_i, [_vp, ctypes.POINTER(_f)]),
+    "arbor_batch_view_buffers": (_i, [_vp, _i, ctypes.POINTER(EngineBuffers)]),
+    "arbor_batch_inspect": (_i, [_vp, ctypes.POINTER(BatchInfo)]),
+    "arbor_batch_read_pixels": (_i, [_vp, _vp, ctypes.c_size_t]),
+    "arbor_batch_destroy": (_i, [_vp]),
 }
 
 
@@ -200,6 +231,78 @@ class Engine:
     def close(self) -> None:
         if self.handle:
             self._lib.arbor_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Owner of an arbor_batch handle (include/arbor.h batched rendering).
+
+    views: (scene index, width, height, C[64]) per view."""
+
+    def __init__(self, seeds, views, stream=None):
+        self._lib = lib()
+        self.views = list(views)
+        arr = (BatchView * len(self.views))()
+        for i, (scene, w, h, C) in enumerate(self.views):
+            arr[i].scene, arr[i].width, arr[i].height = int(scene), int(w), int(h)
+            arr[i].C[:] = [float(x) for x in C]
+        sd = (_i * len(seeds))(*[int(s) for s in seeds])
+        h = _vp()
+        check(self._lib.arbor_batch_create(ctypes.byref(h), sd, len(seeds), arr, len(self.views), stream_handle(stream)))
+        self.handle = h
+
+    def _call(self, name, *args):
+        check(getattr(self._lib, name)(self.handle, *args))
+
+    def render(self) -> None:
+        self._call("arbor_batch_render")
+
+    def profile(self) -> list[float]:
+        ms = (_f * 4)()
+        self._call("arbor_batch_profile", ms)
+        return list(ms)
+
+    def configure(self, tile_width: int, ctas_per_sm: int, order: int, queue: int) -> None:
+        self._call("arbor_batch_configure", ctypes.byref(BatchConfig(tile_width, ctas_per_sm, order, queue)))
+
+    def config(self) -> dict:
+        c = BatchConfig()
+        self._call("arbor_batch_get_config", ctypes.byref(c))
+        return c.as_dict()
+
+    def autotune(self, sample_views: int = 0) -> tuple[dict, list[float]]:
+        best, ms = BatchConfig(), (_f * 16)()
+        self._call("arbor_batch_autotune", sample_views, ctypes.byref(best), ms)
+        return best.as_dict(), list(ms)
+
+    def set_cameras(self, C) -> None:
+        import numpy as np
+
+        flat = np.ascontiguousarray(C, np.float32).reshape(-1)
+        self._call("arbor_batch_set_cameras", flat.ctypes.data_as(ctypes.POINTER(_f)), flat.size // 64)
+
+    def inspect(self) -> BatchInfo:
+        info = BatchInfo()
+        self._call("arbor_batch_inspect", ctypes.byref(info))
+        return info
+
+    def buffers(self, view: int) -> EngineBuffers:
+        b = EngineBuffers()
+        self._call("arbor_batch_view_buffers", view, ctypes.byref(b))
+        return b
+
+    def read_pixels_into(self, host_ptr: int, count: int) -> None:
+        self._call("arbor_batch_read_pixels", host_ptr, count)
+
+    def close(self) -> None:
+        if self.handle:
+            self._lib.arbor_batch_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -30,7 +30,8 @@ enum WorkEvent {
   kEvNewtonStart = 9,  // leaf test that reaches the Newton solve
   kEvNewton = 10,      // Newton iteration (five height-field evaluations)
   kEvStone = 11,       // stone ellipsoid test
-  kEvCount = 12
+  kEvSegment = 12,     // shadow-ray segment toward the sun (forest or tree trace set up)
+  kEvCount = 13
 };
 
 // ------------------------------------------------------------ records --

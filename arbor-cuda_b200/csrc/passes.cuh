@@ -30,7 +30,8 @@ struct PrimaryPolicy {
 };
 
 // Primary rays of one tile (tracePixels, Arbor.cu:252).
-__device__ __forceinline__ void trace_tile(const TraceCtx& c, const Camera& cam, WarpBatch& b, float* __restrict__ Hit, int width, int height,
+template <class WB>
+__device__ __forceinline__ void trace_tile(const TraceCtx& c, const Camera& cam, WB& b, float* __restrict__ Hit, int width, int height,
                                            int x0, int y0, int tw) {
   int x, y;
   tile_pixel_at(threadIdx.x, x0, y0, tw, x, y);
@@ -345,8 +346,8 @@ struct ShadePolicy {
 };
 
 // One tile of shadePixels (Arbor.cu:277-289); c is the shadow-ray context.
-template <bool kForestScene>
-__device__ __forceinline__ void shade_tile(const TraceCtx& c, const Camera& cam, const Instance* inst, WarpBatch& b, const float* __restrict__ P,
+template <bool kForestScene, class WB>
+__device__ __forceinline__ void shade_tile(const TraceCtx& c, const Camera& cam, const Instance* inst, WB& b, const float* __restrict__ P,
                                            const float* __restrict__ Hit, float* __restrict__ Linear, float* __restrict__ Guide, int width,
                                            int height, int x0, int y0, int tw) {
   int x, y;
@@ -379,6 +380,19 @@ constexpr int kSX = kFX + 2 * kHalo, kSY = kFY + 2 * kHalo;
 // Arbor.cu:303
 __device__ __forceinline__ float aces(float x) { return sat((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f)); }
 
+// One channel of resolvePixels' output byte (Arbor.cu:304, packRGB :49):
+// (uint)(sat(pow(c, 1/2.2) * vig) * 255 + 0.5).  The power is the float of
+// the double-precision pow (xpow); CUDA's single-precision powf is within a
+// few ulp of it, which moves the byte only when the scaled value lies within
+// about 1e-4 of a rounding boundary, so powf's byte is used unless the value
+// is within 1e-3 of one, where xpow decides.  Same bytes, cheaper on average.
+__device__ __forceinline__ uint32_t gamma_byte(float c, float vig) {
+  float t = sat(powf(c, 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
+  const float fr = t - floorf(t);
+  if (fr < 1e-3f || fr > 1.0f - 1e-3f) t = sat(xpow(c, 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
+  return (uint32_t)t;
+}
+
 // Arbor.cu:304, one pixel.
 __device__ __forceinline__ void resolve_px(f3 current, float* __restrict__ History, uint32_t* __restrict__ Pixels, float c9, float c10,
                                            float exposure, int x, int y, int width, int height) {
@@ -389,32 +403,58 @@ __device__ __forceinline__ void resolve_px(f3 current, float* __restrict__ Histo
   reinterpret_cast<float4*>(History)[i] = make_float4(mean.x, mean.y, mean.z, count + 1.0f);
   f3 col = mean * exposure;
   col = mk(aces(col.x), aces(col.y), aces(col.z));
-  col = mk(xpow(col.x, 1.0f / 2.2f), xpow(col.y, 1.0f / 2.2f), xpow(col.z, 1.0f / 2.2f));
   float u = ((float)x / (float)width - 0.5f) * 2.0f;
   float v = ((float)y / (float)height - 0.5f) * 2.0f;
-  col = col * (1.0f - 0.09f * (u * u + v * v));
-  Pixels[i] = pack_rgb(col);
+  const float vig = 1.0f - 0.09f * (u * u + v * v);
+  Pixels[i] = gamma_byte(col.x, vig) | (gamma_byte(col.y, vig) << 8) | (gamma_byte(col.z, vig) << 16) | 4278190080u;
 }
 
 // Same-surface 5x5 demodulated filter (Arbor.cu:292-302) of one 32x8 tile,
 // staged with a 2-pixel halo in shared memory so each input pixel is read
-// from HBM once per tile.  kResolve fuses resolvePixels on the filtered value.
-// Threads are laid out 32 x 8 (threadIdx.x, threadIdx.y).
+// from HBM once per tile.  Each halo pixel is staged once as its same-surface
+// key (depth, (int) primitive id, (int) tree id) and its demodulated colour
+// Linear / (Guide + 0.02): the same conversions and IEEE quotients the
+// reference evaluates per neighbour, evaluated once per pixel.  The 5x5 loop
+// is unrolled in the reference's order (rows, then columns) with its weights
+// as constants; tiles whose halo lies inside the image skip the bounds test.
+// kResolve fuses resolvePixels on the filtered value.  Threads are laid out
+// 32 x 8 (threadIdx.x, threadIdx.y).
 struct FilterTile {
-  float4 hit[kSY][kSX];
-  float3 lin[kSY][kSX];
-  float3 gui[kSY][kSX];
-  float w[5];
+  int4 key[kSY][kSX];      // depth bits, primitive id, tree id
+  float4 demod[kSY][kSX];  // Linear / (Guide + 0.02)
+  float w[6];              // weights of r^2 = 0, 1, 2, 4, 5, 8
 };
+
+template <bool kEdge>
+__device__ __forceinline__ void filter_gather(const FilterTile& s, int cx, int cy, int x, int y, int width, int height, int id, int tree,
+                                              float depth, float tol, const float (&w)[6], f3& sum, float& weight) {
+#pragma unroll
+  for (int j = -2; j <= 2; j++)
+#pragma unroll
+    for (int k = -2; k <= 2; k++) {
+      if (kEdge) {
+        int xx = x + k, yy = y + j;
+        if (xx < 0 || yy < 0 || xx >= width || yy >= height) continue;
+      }
+      const int4 q = s.key[cy + j][cx + k];
+      if (q.y != id || q.z != tree || fabsf(__int_as_float(q.x) - depth) > tol) continue;
+      const int r2 = j * j + k * k;
+      const float wt = w[r2 == 0 ? 0 : r2 == 1 ? 1 : r2 == 2 ? 2 : r2 == 4 ? 3 : r2 == 5 ? 4 : 5];
+      const float4 d = s.demod[cy + j][cx + k];
+      sum = sum + mk(d.x, d.y, d.z) * wt;
+      weight += wt;
+    }
+}
+
 template <bool kResolve>
 __device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restrict__ Linear, const float* __restrict__ Guide,
                                             const float* __restrict__ Hit, float* __restrict__ Filtered, float* __restrict__ History,
                                             uint32_t* __restrict__ Pixels, float c9, float c10, float c15, float c20, int width, int height,
                                             int x0, int y0) {
   const int tid = threadIdx.y * kFX + threadIdx.x;
-  // Filter weights expf(-(j*j+k*k)*0.30f) for the 5 distinct radii 1,2,4,5,8.
-  if (tid < 5) {
-    const int r2[5] = {1, 2, 4, 5, 8};
+  // Filter weights expf(-(j*j+k*k)*0.30f) for r^2 = 0, 1, 2, 4, 5, 8.
+  if (tid < 6) {
+    const int r2[6] = {0, 1, 2, 4, 5, 8};
     s.w[tid] = xexp(-(float)r2[tid] * 0.30f);
   }
   const int hx0 = x0 - kHalo, hy0 = y0 - kHalo;
@@ -423,44 +463,37 @@ __device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restri
     int gx = hx0 + sx, gy = hy0 + sy;
     if (gx >= 0 && gy >= 0 && gx < width && gy < height) {
       int q = gy * width + gx;
-      s.hit[sy][sx] = __ldg(reinterpret_cast<const float4*>(Hit) + q);
+      float4 h = __ldg(reinterpret_cast<const float4*>(Hit) + q);
       float4 l = __ldg(reinterpret_cast<const float4*>(Linear) + q);
       float4 g = __ldg(reinterpret_cast<const float4*>(Guide) + q);
-      s.lin[sy][sx] = make_float3(l.x, l.y, l.z);
-      s.gui[sy][sx] = make_float3(g.x, g.y, g.z);
+      s.key[sy][sx] = make_int4(__float_as_int(h.x), (int)h.y, (int)h.z, 0);
+      s.demod[sy][sx] = make_float4(l.x / (g.x + 0.02f), l.y / (g.y + 0.02f), l.z / (g.z + 0.02f), 0.0f);
     }
   }
   __syncthreads();
   const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
   if (x < width && y < height) {
     const int cx = threadIdx.x + kHalo, cy = threadIdx.y + kHalo;
-    float4 hb = s.hit[cy][cx];
-    float3 lc = s.lin[cy][cx], gc = s.gui[cy][cx];
+    const int i = y * width + x;
+    const int4 kc = s.key[cy][cx];
+    const float depth = __int_as_float(kc.x);
+    float4 lc = __ldg(reinterpret_cast<const float4*>(Linear) + i);
     f3 col = mk(lc.x, lc.y, lc.z);
-    f3 base = mk(gc.x, gc.y, gc.z) + mk(0.02f, 0.02f, 0.02f);
-    f3 sum = mk(0.0f, 0.0f, 0.0f);
-    float weight = 0.0f;
-    int id = (int)hb.y;
-    float depth = hb.x;
     if (depth < kFar && c15 < 0.5f) {
-      int treeB = (int)hb.z;
-      float tol = fmaxf(0.005f, hb.w * 6.0f);
-      for (int j = -2; j <= 2; j++)
-        for (int k = -2; k <= 2; k++) {
-          int xx = x + k, yy = y + j;
-          if (xx < 0 || yy < 0 || xx >= width || yy >= height) continue;
-          float4 hq = s.hit[cy + j][cx + k];
-          if ((int)hq.y != id || (int)hq.z != treeB || fabsf(hq.x - depth) > tol) continue;
-          int r2 = j * j + k * k;
-          float w = r2 == 0 ? 1.0f : s.w[r2 == 1 ? 0 : r2 == 2 ? 1 : r2 == 4 ? 2 : r2 == 5 ? 3 : 4];
-          float3 c = s.lin[cy + j][cx + k], g3 = s.gui[cy + j][cx + k];
-          f3 g = mk(g3.x, g3.y, g3.z) + mk(0.02f, 0.02f, 0.02f);
-          sum = sum + mk(c.x / g.x, c.y / g.y, c.z / g.z) * w;
-          weight += w;
-        }
+      float4 gc = __ldg(reinterpret_cast<const float4*>(Guide) + i);
+      f3 base = mk(gc.x, gc.y, gc.z) + mk(0.02f, 0.02f, 0.02f);
+      f3 sum = mk(0.0f, 0.0f, 0.0f);
+      float weight = 0.0f;
+      const float tol = fmaxf(0.005f, __ldg(Hit + 4 * i + 3) * 6.0f);
+      const float w[6] = {s.w[0], s.w[1], s.w[2], s.w[3], s.w[4], s.w[5]};
+      const bool interior = x0 >= kHalo && y0 >= kHalo && x0 + kFX + kHalo <= width && y0 + kFY + kHalo <= height;
+      if (interior)
+        filter_gather<false>(s, cx, cy, x, y, width, height, kc.y, kc.z, depth, tol, w, sum, weight);
+      else
+        filter_gather<true>(s, cx, cy, x, y, width, height, kc.y, kc.z, depth, tol, w, sum, weight);
       if (weight > 0.0f) col = mix3(col, (sum / weight) * base, 0.86f);
     }
-    reinterpret_cast<float4*>(Filtered)[y * width + x] = make_float4(col.x, col.y, col.z, 1.0f);
+    reinterpret_cast<float4*>(Filtered)[i] = make_float4(col.x, col.y, col.z, 1.0f);
     if (kResolve) resolve_px(col, History, Pixels, c9, c10, c20, x, y, width, height);
   }
 }

@@ -4,7 +4,7 @@
 // (Arbor.cu:226).  On a GPU that serialises a warp: the rare, long tests
 // (the leaf Newton solve, the bark SDF march) run with one or two lanes
 // active.  Here each lane traverses on its own (tracer.cuh) and, instead of
-// testing a candidate, queues it (up to kQueue per lane) and keeps
+// testing a candidate, queues it (up to Q per lane) and keeps
 // traversing; when every lane is blocked (queue full, tree finished, ray
 // done) the warp runs all queued tests as compacted jobs - leaf clips, then
 // Newton solves of the clips that pass, wood tests and the rest - one job per
@@ -26,15 +26,18 @@
 
 namespace arbor {
 
-constexpr int kQueue = 8;        // candidates a lane may queue
-constexpr int kWarpJobs = 32 * kQueue;
+constexpr int kQueue = 8;        // default candidates a lane may queue
 constexpr int kNewtonCap = 64;   // pending Newton solves per warp
 
-struct WarpBatch {
+// Per-warp shared-memory batch for a queue depth of Q candidates per lane.
+template <int Q>
+struct WarpBatchQ {
+  static constexpr int kQ = Q;
+  static constexpr int kWarpJobs = 32 * Q;
   float4 rayO[32];             // owner lane's local ray origin and wind time
   float4 rayD[32];             // owner lane's local ray direction
   LeafSolve solve[kNewtonCap];
-  int prim[kWarpJobs];         // lane-major queue: lane * kQueue + k
+  int prim[kWarpJobs];         // lane-major queue: lane * Q + k
   float fp[kWarpJobs];
   int type[kWarpJobs];
   float res[kWarpJobs];
@@ -43,10 +46,12 @@ struct WarpBatch {
   short miscJob[kWarpJobs];
   short solveJob[kNewtonCap];
 };
+using WarpBatch = WarpBatchQ<kQueue>;
 
 // Advance one lane until its queue is full, its tree is finished with tests
 // pending, or its ray is done.
-__device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WarpBatch& b, int lane, int& nq) {
+template <class WB>
+__device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WB& b, int lane, int& nq) {
   while (r.phase == kPhDDA || r.phase == kPhTree || r.phase == kPhLeaf || r.phase == kPhTreeEnd) {
     if (r.phase == kPhDDA) {
       dda_step(c, r);
@@ -64,11 +69,11 @@ __device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WarpBat
     // an accepted leaf: queue its primitive
     uint32_t uid = __ldg(c.Order + (r.node - kCapacity));
     if (uid < (uint32_t)kCapacity) {  // an Order entry past the records is skipped, not read
-      int q = lane * kQueue + nq++;
+      int q = lane * WB::kQ + nq++;
       b.prim[q] = (int)uid;
       b.fp[q] = fmaxf(0.000005f, r.lcone * fmaxf(0.05f, r.spanx));
       b.type[q] = (int)ldg4(c.P, (int)uid * 6).w;
-      if (nq == kQueue) {
+      if (nq == WB::kQ) {
         r.phase = kPhBlocked;  // resume with the pop once results are in
         return;
       }
@@ -85,7 +90,8 @@ __device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WarpBat
 }
 
 // Run every queued test of the warp.  All 32 lanes call it together.
-__device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WarpBatch& b, int lane, int nq) {
+template <class WB>
+__device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB& b, int lane, int nq) {
   const unsigned full = 0xffffffffu;
   const unsigned lt = (1u << lane) - 1u;
   if (nq > 0) {
@@ -95,7 +101,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, War
   // per-lane counts by class, scanned across the warp
   int nl = 0, nw = 0, nm = 0;
   for (int k = 0; k < nq; k++) {
-    int t = b.type[lane * kQueue + k];
+    int t = b.type[lane * WB::kQ + k];
     if (t == 1)
       nl++;
     else if (t == 0 && c.refine)
@@ -116,7 +122,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, War
   const int totL = __shfl_sync(full, sl, 31), totW = __shfl_sync(full, sw, 31), totM = __shfl_sync(full, sm, 31);
   int ol = sl - nl, ow = sw - nw, om = sm - nm;
   for (int k = 0; k < nq; k++) {
-    int q = lane * kQueue + k;
+    int q = lane * WB::kQ + k;
     int t = b.type[q];
     if (t == 1)
       b.leafJob[ol++] = (short)q;
@@ -135,7 +141,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, War
     int q = 0;
     if (j < totL) {
       q = b.leafJob[j];
-      int owner = q / kQueue;
+      int owner = q / WB::kQ;
       float4 o = b.rayO[owner], d = b.rayD[owner];
       solve = leaf_clip(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls);
       if (!solve) b.res[q] = ls.best;
@@ -169,7 +175,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, War
     int j = base + lane;
     if (j < totW) {
       int q = b.woodJob[j];
-      int owner = q / kQueue;
+      int owner = q / WB::kQ;
       float4 o = b.rayO[owner], d = b.rayD[owner];
       b.res[q] = wood_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], true);
     }
@@ -179,7 +185,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, War
     int j = base + lane;
     if (j < totM) {
       int q = b.miscJob[j];
-      int owner = q / kQueue;
+      int owner = q / WB::kQ;
       float4 o = b.rayO[owner], d = b.rayD[owner];
       b.res[q] = object_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], o.w, c.wind, c.refine);
     }
@@ -188,12 +194,13 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, War
 }
 
 // Apply a lane's results in candidate order and resume it.
-__device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, const WarpBatch& b, int lane, int& nq) {
+template <class WB>
+__device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, const WB& b, int lane, int& nq) {
   for (int k = 0; k < nq; k++) {
-    float t = b.res[lane * kQueue + k];
+    float t = b.res[lane * WB::kQ + k];
     if (t < r.lbest) {
       r.lbest = t;
-      r.lfound = b.prim[lane * kQueue + k];
+      r.lfound = b.prim[lane * WB::kQ + k];
     }
   }
   nq = 0;
@@ -209,8 +216,8 @@ __device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, const War
 
 // Drive one warp's rays to completion.  Policy::done(r) is called for a
 // finished ray and either starts a new trace on r or sets it idle.
-template <class Policy>
-__device__ __forceinline__ void batch_run(const TraceCtx& c, Ray& r, WarpBatch& b, Policy& policy) {
+template <class WB, class Policy>
+__device__ __forceinline__ void batch_run(const TraceCtx& c, Ray& r, WB& b, Policy& policy) {
   const int lane = threadIdx.x & 31;
   int nq = 0;
   for (;;) {

@@ -44,35 +44,57 @@ WEIGHTS = {
     "newton": 140,
     # stone ellipsoid (Arbor.cu:219)
     "stone": 32,
+    # shadow segment: world-box clip and DDA setup of traceForest, transmission and origin update (Arbor.cu:239-244, 272)
+    "segment": 70,
 }
-EVENTS = ["ray", "cell", "tree", "node", "wood", "march", "bark", "wood_shadow", "leaf", "newton_start", "newton", "stone"]
+EVENTS = ["ray", "cell", "tree", "node", "wood", "march", "bark", "wood_shadow", "leaf", "newton_start", "newton", "stone", "segment"]
 
 
-def count_events(ab, P, Nodes, Order, C, width: int, height: int, single_tree: bool, torch) -> dict:
+def count_events(ab, P, Nodes, Order, C, width: int, height: int, single_tree: bool, torch, Hit=None) -> dict:
+    """Event totals of one tracePixels launch, or of one shadePixels launch
+    on the Hit records `Hit` when given."""
     n = int(ab.lib().arbor_trace_work_slots(width, height))
     slots = torch.zeros(n, dtype=torch.int32, device="cuda")
-    st = ab.call("arbor_traceWork", P, Nodes, Order, C, width, height, int(single_tree), slots)
+    if Hit is None:
+        st = ab.call("arbor_traceWork", P, Nodes, Order, C, width, height, int(single_tree), slots)
+    else:
+        st = ab.call("arbor_shadeWork", P, Nodes, Order, C, Hit, width, height, int(single_tree), slots)
     if st != ab.OK:
         raise RuntimeError(ab.last_error())
     per = slots.view(-1, 16).to(torch.int64).sum(0).cpu().numpy()
     return {name: int(per[i]) for i, name in enumerate(EVENTS)}
 
 
+def add_counts(a: dict, b: dict) -> dict:
+    return {k: a.get(k, 0) + b.get(k, 0) for k in EVENTS}
+
+
 def flops(counts: dict) -> int:
     return int(sum(WEIGHTS[k] * counts[k] for k in EVENTS))
 
 
-def trace_roofline(ab, fr, torch, ms_trace: float, fp32_peak_tops: float, sm_clock_mhz: float) -> dict:
-    counts = count_events(ab, fr.P, fr.Nodes, fr.Order, fr.C, fr.w, fr.h, fr.spec["single_tree"], torch)
+def roofline_entry(kernel: str, counts: dict, pixels: int, ms: float, fp32_peak_tops: float, sm_clock_mhz: float) -> dict:
+    """FP32 roofline line of one launch whose counted events are `counts`
+    over `pixels` pixels, timed at `ms` per launch."""
     ops = flops(counts)
-    achieved = ops / (ms_trace / 1e3) / 1e12
-    rays = max(1, counts["ray"])
+    achieved = ops / (ms / 1e3) / 1e12
+    pixels = max(1, pixels)
     return {
-        "kernel": "tracePixels", "bound": "fp32", "achieved": round(achieved, 3), "peak": round(fp32_peak_tops, 2),
+        "kernel": kernel, "bound": "fp32", "achieved": round(achieved, 3), "peak": round(fp32_peak_tops, 2),
         "unit": "TFLOP/s", "frac": round(achieved / fp32_peak_tops, 4), "traffic": None,
-        "algorithmic_flops": ops, "flops_per_ray": round(ops / rays, 1),
-        "events_per_ray": {k: round(v / rays, 3) for k, v in counts.items()},
+        "algorithmic_flops": ops, "flops_per_pixel": round(ops / pixels, 1),
+        "events_per_pixel": {k: round(v / pixels, 3) for k, v in counts.items() if v},
         "peak_source": f"derived: 148 SM x 128 FP32 lanes x {sm_clock_mhz:.0f} MHz measured SM clock, one non-fused op per lane per "
                        "cycle (no FP32 peak in MEASURED_PEAKS.json)",
-        "ms_per_launch": round(ms_trace, 4),
+        "ms_per_launch": round(ms, 4),
     }
+
+
+def trace_roofline(ab, fr, torch, ms_trace: float, fp32_peak_tops: float, sm_clock_mhz: float) -> dict:
+    counts = count_events(ab, fr.P, fr.Nodes, fr.Order, fr.C, fr.w, fr.h, fr.spec["single_tree"], torch)
+    return roofline_entry("tracePixels", counts, fr.w * fr.h, ms_trace, fp32_peak_tops, sm_clock_mhz)
+
+
+def shade_roofline(ab, fr, torch, ms_shade: float, fp32_peak_tops: float, sm_clock_mhz: float) -> dict:
+    counts = count_events(ab, fr.P, fr.Nodes, fr.Order, fr.C, fr.w, fr.h, fr.spec["single_tree"], torch, Hit=fr.Hit)
+    return roofline_entry("shadePixels", counts, fr.w * fr.h, ms_shade, fp32_peak_tops, sm_clock_mhz)

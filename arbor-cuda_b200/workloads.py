@@ -103,3 +103,56 @@ def shadow_sun(seed: int = FOREST_SEED) -> tuple[float, float]:
 
 
 VIEW_PRESETS = (1, 2, 3, 4, 5)
+
+
+BATCH_RESOLUTIONS = ((320, 180), (640, 360), (1280, 720), (1920, 1080))
+
+
+def batch_seeds(n: int, seed: int = FOREST_SEED) -> list[int]:
+    """n master seeds: `seed` first, then seeds drawn from rnd(k, seed) over
+    the engine's seed range 0..1,000,000 (src/engine.js:28)."""
+    out = [seed]
+    k = 1
+    while len(out) < n:
+        s = int(rnd(k, seed) * 1000000.0)
+        if s not in out:
+            out.append(s)
+        k += 1
+    return out
+
+
+def view_pose_state(scene_seed: int, width: int, height: int, eye_x: float, eye_z: float, yaw: float, pitch: float,
+                    shadows: bool = True) -> np.ndarray:
+    """Camera/state record of a first-person view at (eye_x, 1.72, eye_z)
+    looking along (yaw, pitch), as fpsPose lays it out (Arbor.cu:179): the
+    look-at point is the eye plus the unit view direction; first sample with
+    history reset; sun shadows at 35 degrees elevation, azimuth from the seed."""
+    C = base_state(scene_seed, width, height)
+    eye = np.array([eye_x, 1.72, eye_z], np.float64)
+    f = np.array([math.sin(yaw) * math.cos(pitch), math.sin(pitch), math.cos(yaw) * math.cos(pitch)])
+    C[0:3] = eye
+    C[4:7] = eye + f
+    C[16] = C[27] = yaw
+    C[17] = C[28] = pitch
+    C[22] = 1.0 if shadows else 0.0
+    if shadows:
+        C[12], C[13] = shadow_sun(scene_seed)
+    C[9], C[10] = 0.0, 1.0
+    return C
+
+
+def batch_views(n_views: int, seeds: list[int], resolutions=BATCH_RESOLUTIONS, seed: int = FOREST_SEED, shadows: bool = True,
+                extent: float = 200.0) -> list[tuple[int, int, int, np.ndarray]]:
+    """(scene index, width, height, C) of n_views seeded views: resolution
+    uniform over `resolutions`, scene uniform over the seeds, eye uniform in
+    the forest square [-extent, extent]^2 at 1.72 m, yaw uniform, pitch
+    uniform in [-0.05, 0.20] rad."""
+    out = []
+    for v in range(n_views):
+        r = [rnd(1000 + 8 * v + k, seed) for k in range(6)]
+        w, h = resolutions[min(int(r[0] * len(resolutions)), len(resolutions) - 1)]
+        scene = min(int(r[1] * len(seeds)), len(seeds) - 1)
+        C = view_pose_state(seeds[scene], w, h, (r[2] * 2.0 - 1.0) * extent, (r[3] * 2.0 - 1.0) * extent, r[4] * 2.0 * math.pi,
+                            -0.05 + 0.25 * r[5], shadows)
+        out.append((scene, w, h, C))
+    return out

@@ -45,7 +45,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="arbor", choices=["arbor", "reference"])
-    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "wind", "tree"])
+    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "wind", "tree", "batch"])
+    ap.add_argument("--views", type=int, default=64, help="batch workload: views per batch")
+    ap.add_argument("--scenes", type=int, default=16, help="batch workload: resident scenes (master seeds)")
+    ap.add_argument("--tune-views", type=int, default=8, help="batch workload: views the autotuner times each configuration on")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--width", type=int, default=0, help="override the workload's width (profiling runs)")
@@ -307,12 +310,13 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
-    try:
-        import roofline_model
+    import roofline_model
 
-        result["roofline"] = roofline_model.trace_roofline(ab, fr, torch, ms_trace, fp32_peak, sm_clock)
-    except ImportError:
-        pass
+    # The FP32 roofline of the dominant kernel (trace, or shade when sun
+    # shadows make it the longer pass); both are reported.
+    result["roofline_trace"] = roofline_model.trace_roofline(ab, fr, torch, ms_trace, fp32_peak, sm_clock)
+    result["roofline_shade"] = roofline_model.shade_roofline(ab, fr, torch, ms_shade, fp32_peak, sm_clock)
+    result["roofline"] = result["roofline_trace"] if ms_trace >= ms_shade else result["roofline_shade"]
 
     # End to end through the engine API with host buffers.
     if not args.no_e2e:
@@ -442,6 +446,9 @@ def cpu_baseline(spec: dict, target_s: float) -> dict:
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
+    if args.workload == "batch":
+        run_reference_batch(args)
+        return
     spec = workload_spec(args.workload)
     if args.width and args.height:
         spec.update(width=args.width, height=args.height)
@@ -468,6 +475,184 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------ batch views --
+def batch_spec(args) -> dict:
+    return {"workload": f"batch-{args.views}-views: {args.views} views of {args.scenes} resident forests (324 trees each, master seeds "
+                        "7 and seeded draws), resolutions uniform over 320x180/640x360/1280x720/1920x1080, seeded poses inside the "
+                        "forest at 1.72 m, 1 spp, sun shadows on; one CUDA graph launch per batch",
+            "views": args.views, "scenes": args.scenes, "spp": 1, "shadows": True}
+
+
+def run_batch(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    import torch.distributed as dist
+
+    import arbor_b200 as ab
+    import roofline_model
+    import workloads
+
+    spec = batch_spec(args)
+    seeds = workloads.batch_seeds(args.scenes)
+    views = workloads.batch_views(args.views, seeds)
+    stream = torch.cuda.current_stream()
+    b = ab.Batch(seeds, views, stream=stream)
+    try:
+        info = b.inspect()
+        total_px = int(info.total_pixels)
+        t0 = time.perf_counter()
+        best, table = b.autotune(args.tune_views)
+        tune_s = time.perf_counter() - t0
+        for _ in range(args.warmup):
+            b.render()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        sampler = ClockSampler(physical_gpu(local_rank))
+        sampler.start()
+        time.sleep(0.3)
+        launches0 = ab.launches()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            b.render()
+        end.record()
+        end.synchronize()
+        launches = ab.launches() - launches0
+        clocks = sampler.stop()
+        t = torch.tensor([start.elapsed_time(end)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dist.barrier()
+        ms_max = float(t.item())
+        value = world * total_px * args.steps / (ms_max / 1e3) / 1e6
+
+        # Per-kernel durations: the graph's kernels launched one by one.
+        prof = [b.profile() for _ in range(2)][-1]
+        ms_setup, ms_trace, ms_shade, ms_filter = prof
+        peaks = measured_peaks()
+        hbm_peak = peaks.get("hbm_gbs")
+        sm_clock = clocks.get("sm_mhz") or peaks.get("clocks_under_load", {}).get("sm_mhz_median") or 1965.0
+        fp32_peak = 148 * 128 * sm_clock * 1e6 / 1e12
+        tc, sc = {}, {}
+        for v, (_, w, h, _) in enumerate(views):
+            buf = b.buffers(v)
+            tc = roofline_model.add_counts(tc, roofline_model.count_events(ab, buf.P, buf.Nodes, buf.Order, buf.C, w, h, False, torch))
+            sc = roofline_model.add_counts(sc, roofline_model.count_events(ab, buf.P, buf.Nodes, buf.Order, buf.C, w, h, False, torch, Hit=buf.Hit))
+        r_trace = roofline_model.roofline_entry("batch trace pass (tracePixels of every view)", tc, total_px, ms_trace, fp32_peak, sm_clock)
+        r_shade = roofline_model.roofline_entry("batch shade pass (shadePixels of every view)", sc, total_px, ms_shade, fp32_peak, sm_clock)
+        # first sample of every view (history reset): Linear, Guide, Hit read, Filtered and History written, Pixels written
+        fr_bytes = total_px * (48 + 16 + 16 + 4)
+        fr_gbs = fr_bytes / (ms_filter / 1e3) / 1e9
+        result = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: procedural scenes grown from the master seeds; seeded poses (no dataset)",
+            "config": {**spec, "total_pixels": total_px, "parallelism": f"replicas x{world}",
+                       "resolutions": {f"{w}x{h}": sum(1 for v in views if (v[1], v[2]) == (w, h)) for w, h in workloads.BATCH_RESOLUTIONS},
+                       "l2": f"per-step images ({total_px * 84 / 1e9:.2f} GB) far exceed the 126 MB L2"},
+            "autotune": {"chosen": best, "sample_views": args.tune_views, "seconds": round(tune_s, 2),
+                         "ms_per_config": {f"tw{tw}_ctas{c}_order{o}_q{q}": round(table[i], 3)
+                                           for i, (tw, c, o, q) in enumerate((tw, c, o, q) for tw in (16, 32) for c in (1, 2)
+                                                                             for o in (0, 1) for q in (4, 8))}},
+            "phases_ms": {"setup": round(ms_setup, 4), "trace": round(ms_trace, 4), "shade": round(ms_shade, 4),
+                          "filter_resolve": round(ms_filter, 4)},
+            "roofline": r_trace if ms_trace >= ms_shade else r_shade, "roofline_trace": r_trace, "roofline_shade": r_shade,
+            "roofline_hbm": {"kernel": "batch filter+resolve pass", "bound": "hbm", "achieved": round(fr_gbs, 1), "peak": hbm_peak,
+                             "unit": "GB/s", "frac": round(fr_gbs / hbm_peak, 4) if hbm_peak else None, "traffic": None,
+                             "algorithmic_bytes": fr_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        if not args.no_e2e:
+            result["e2e"] = batch_e2e(b, torch, views, total_px, args)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_batch_sample(seeds, views, args.cpu_seconds)
+        if rank == 0:
+            print(json.dumps(result), flush=True)
+    finally:
+        b.close()
+
+
+def batch_e2e(b, torch, views, total_px: int, args) -> dict:
+    """Per step: every view's camera record from host memory, one batch
+    render, every view's Pixels back to pinned host memory."""
+    C = np.ascontiguousarray(np.stack([v[3] for v in views]), np.float32)
+    host = torch.empty(total_px, dtype=torch.int32).pin_memory()
+    stream = torch.cuda.current_stream()
+    for _ in range(max(1, args.warmup // 2)):
+        b.set_cameras(C)
+        b.render()
+        b.read_pixels_into(host.data_ptr(), total_px)
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(stream)
+    for _ in range(args.steps):
+        b.set_cameras(C)
+        b.render()
+        b.read_pixels_into(host.data_ptr(), total_px)
+    e.record(stream)
+    e.synchronize()
+    wall = time.perf_counter() - t0
+    ms = a.elapsed_time(e)
+    return {"value": round(total_px * args.steps / (ms / 1e3) / 1e6, 3), "unit": UNIT, "h2d_bytes_per_step": int(C.nbytes),
+            "d2h_bytes_per_step": total_px * 4, "ms_per_step": round(ms / args.steps, 4),
+            "host_wall_ms_per_step": round(wall * 1e3 / args.steps, 4),
+            "api": "arbor_batch_set_cameras + arbor_batch_render + arbor_batch_read_pixels (pinned host buffers)"}
+
+
+def cpu_batch_sample(seeds, views, target_s: float) -> dict:
+    """The reference's CPU implementation on evenly strided rows of four of
+    the batch's views (one of each resolution where the batch has it)."""
+    o, kind = cpu_oracle()
+    picked, seen = [], set()
+    for v in views:
+        if (v[1], v[2]) not in seen:
+            seen.add((v[1], v[2]))
+            picked.append(v)
+    scenes = {}
+    rays = 0
+    secs = 0.0
+    per_view = target_s / len(picked)
+    for scene, w, h, C in picked:
+        if scene not in scenes:
+            scenes[scene] = o.build_scene(seeds[scene])
+        bufs = {k: np.zeros(w * h * 4, np.float32) for k in ("Hit", "Linear", "Guide", "Filtered", "History")}
+        bufs["Pixels"] = np.zeros(w * h, np.uint32)
+        n = min(h, 4 * max(1, o.max_threads()))
+        for attempt in range(2):
+            rows = np.unique((np.arange(n) * h // n + (h // n) // 2).clip(0, h - 1)).astype(np.int32)
+            t0 = time.perf_counter()
+            o.frame_rows(scenes[scene], C.copy(), w, h, rows, bufs)
+            dt = time.perf_counter() - t0
+            if attempt == 0:
+                n = int(min(h, max(len(rows), len(rows) * per_view / max(dt, 1e-3))))
+        rays += len(rows) * w
+        secs += dt
+    return {"value": round(rays / secs / 1e6, 4), "unit": UNIT, "cores": o.max_threads(), "kind": kind,
+            "sample": f"evenly strided rows of {len(picked)} views of the batch ({', '.join(f'{p[1]}x{p[2]}' for p in picked)}; "
+                      f"{rays} primary rays, {secs:.2f} s): trace, shade with sun shadows, filter, resolve",
+            "seconds": round(secs, 3)}
+
+
+def run_reference_batch(args) -> None:
+    import workloads
+
+    seeds = workloads.batch_seeds(args.scenes)
+    views = workloads.batch_views(args.views, seeds)
+    step_s = float(os.environ.get("ARBOR_REFERENCE_STEP_SECONDS", "2.0"))
+    samples = [cpu_batch_sample(seeds, views, step_s) for _ in range(args.warmup + args.steps)][args.warmup:]
+    value = statistics.mean(x["value"] for x in samples)
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * statistics.mean(x["seconds"] for x in samples), 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic: procedural scenes grown from the master seeds", "impl": "reference",
+            "config": batch_spec(args),
+            "cpu_baseline": {k: samples[-1][k] for k in ("unit", "cores", "kind", "sample")} | {"value": round(value, 4)},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -486,7 +671,10 @@ def main() -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
     try:
-        run_arbor(args, rank, world, local_rank)
+        if args.workload == "batch":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_arbor(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

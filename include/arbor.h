@@ -200,10 +200,14 @@ ARBOR_API int arbor_filterResolve(const float* Linear, const float* Guide, const
  * (single_tree != 0) launch performs, per thread, into `slots` (caller-owned,
  * arbor_trace_work_slots(width, height) uint32 values: 16 per thread, events
  * in the order ray, cell, tree, node, wood, march, bark, wood-shadow, leaf,
- * newton-start, newton, stone).  It runs the same code compiled with
+ * newton-start, newton, stone, segment).  It runs the same code compiled with
  * counters and writes no Hit. */
 ARBOR_API size_t arbor_trace_work_slots(int width, int height);
 ARBOR_API int arbor_traceWork(const float* P, const float* Nodes, const uint32_t* Order, const float* C, int width, int height, int single_tree, uint32_t* slots, arbor_stream stream);
+/* The same count for one shadePixels launch on the given Hit records: the
+ * shading's own events (surface normals) and, per shadow segment toward the
+ * sun, event 12 (segment) plus its traversal and primitive-test events. */
+ARBOR_API int arbor_shadeWork(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, int width, int height, int single_tree, uint32_t* slots, arbor_stream stream);
 
 /* ---------------------------------------------------------------------------
  * Engine: the C++ host of src/engine.js (generate / resize / frame /
@@ -253,6 +257,73 @@ ARBOR_API int arbor_engine_read_pixels(arbor_engine* e, uint32_t* host, size_t c
 ARBOR_API int arbor_engine_dispose(arbor_engine* e);
 /* Disposes (if needed) and frees the handle. */
 ARBOR_API int arbor_engine_destroy(arbor_engine* e);
+
+
+/* ---------------------------------------------------------------------------
+ * Batched rendering: many views of many resident scenes, each view with its
+ * own resolution and camera/state record, rendered by one CUDA graph launch
+ * (a per-view setup kernel, persistent trace and shade kernels and a
+ * persistent filter+resolve kernel, all pulling tiles from global queues).
+ * No reference counterpart: the reference renders one view per frame
+ * (src/engine.js:45-53).  Each view renders as arbor_tracePixels +
+ * arbor_shadePixels + arbor_filterResolve render it on the same scene and C.
+ * Forest scenes only.
+ * ------------------------------------------------------------------------- */
+typedef struct arbor_batch arbor_batch;
+
+typedef struct arbor_batch_view {
+  int scene;        /* index into the seeds array given to arbor_batch_create */
+  int width, height;
+  int reserved;
+  float C[64];      /* camera/state record (Arbor.cu:179-182 layout); C[31] is the forest's world seed */
+} arbor_batch_view;
+
+typedef struct arbor_batch_config {
+  int tile_width;   /* trace/shade tile: 16 (16x16 pixels) or 32 (32x8 pixels) */
+  int ctas_per_sm;  /* persistent CTAs per SM: 1 or 2 */
+  int order;        /* tile order: 0 view by view, 1 largest views first */
+  int queue;        /* warp-batch queue depth, candidates per lane: 4 or 8 */
+} arbor_batch_config;
+
+typedef struct arbor_batch_info {
+  int n_scenes, n_views;
+  uint64_t total_pixels;
+  uint64_t allocated_bytes;
+  int trace_tiles, filter_tiles;
+  uint64_t renders;
+  uint32_t launches_per_render;   /* kernels in the graph */
+  arbor_batch_config config;
+} arbor_batch_info;
+
+/* Builds every scene (seeds: integers 0..1,000,000) and allocates every
+ * view's Hit/Linear/Guide/Filtered/History/Pixels on the current device.
+ * The batch works on a stream of its own, ordered after `stream` at each
+ * call, and `stream` is ordered after the work each call queues.  Default
+ * configuration: 16x16 tiles, 2 CTAs/SM, view order, queue depth 8. */
+ARBOR_API int arbor_batch_create(arbor_batch** out, const int* seeds, int n_scenes, const arbor_batch_view* views, int n_views, arbor_stream stream);
+/* Replaces every view's camera record (n_views x 64 floats, host memory). */
+ARBOR_API int arbor_batch_set_cameras(arbor_batch* b, const float* C, int n_views);
+ARBOR_API int arbor_batch_configure(arbor_batch* b, const arbor_batch_config* cfg);
+ARBOR_API int arbor_batch_get_config(arbor_batch* b, arbor_batch_config* cfg);
+/* Times the trace and shade kernels of every configuration (16, ordered by
+ * tile_width, ctas_per_sm, order, queue, the last varying fastest) on
+ * `sample_views` views spread over the batch (all when <= 0), writes the
+ * times to ms_table (nullable, 16 floats), keeps the fastest and returns it
+ * in best (nullable).  The sample renders overwrite those views' Hit,
+ * Linear and Guide. */
+ARBOR_API int arbor_batch_autotune(arbor_batch* b, int sample_views, arbor_batch_config* best, float* ms_table);
+/* Renders every view: one graph launch. */
+ARBOR_API int arbor_batch_render(arbor_batch* b);
+/* Renders every view with the graph's four kernels launched one by one and
+ * writes each one's duration (CUDA events, ms) to ms4: setup, trace, shade,
+ * filter+resolve. */
+ARBOR_API int arbor_batch_profile(arbor_batch* b, float* ms4);
+/* Device buffers of one view (its scene's records, its C record and images). */
+ARBOR_API int arbor_batch_view_buffers(arbor_batch* b, int view, arbor_engine_buffers* out);
+ARBOR_API int arbor_batch_inspect(arbor_batch* b, arbor_batch_info* info);
+/* Copies every view's Pixels, view after view, into host memory and waits. */
+ARBOR_API int arbor_batch_read_pixels(arbor_batch* b, uint32_t* host, size_t count);
+ARBOR_API int arbor_batch_destroy(arbor_batch* b);
 
 #ifdef __cplusplus
 }

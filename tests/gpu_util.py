@@ -1,4 +1,6 @@
 """Device-buffer helpers for the GPU tests (torch is only the allocator)."""
+import ctypes
+
 import numpy as np
 import torch
 
@@ -66,3 +68,35 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return np.abs(a - b) / np.maximum(1.0, np.abs(b))
+
+
+_RT = None
+
+
+def _cudart():
+    """The CUDA runtime torch itself loaded (used only to copy library-owned buffers out)."""
+    global _RT
+    if _RT is None:
+        import glob
+        import os
+
+        base = os.path.join(os.path.dirname(torch.__file__), "..", "nvidia")
+        cands = sorted(glob.glob(os.path.join(base, "cuda_runtime", "lib", "libcudart.so*")))
+        cands += ["libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so"]
+        for c in cands:
+            try:
+                _RT = ctypes.CDLL(c)
+                break
+            except OSError:
+                continue
+        _RT.cudaMemcpy.restype = ctypes.c_int
+        _RT.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    return _RT
+
+
+def dev_array(ptr: int, n: int, dtype=np.float32) -> np.ndarray:
+    """Copy n 4-byte elements at a library-owned device address to the host."""
+    torch.cuda.synchronize()
+    out = np.empty(n, dtype)
+    assert _cudart().cudaMemcpy(out.ctypes.data, ptr, n * 4, 2) == 0  # cudaMemcpyDeviceToHost
+    return out

@@ -88,6 +88,10 @@ def test_scalar_ranges(lib):
     assert lib.arbor_reduceBounds(A, 0, None) == ab.OK  # nothing to reduce: no launch
     assert lib.arbor_updateCamera(A, A + MB, A + 2 * MB, float("nan"), 64, 64, None) == ab.ERR_VALUE
     assert lib.arbor_updateCamera(A, A + MB, A + 2 * MB, float("inf"), 64, 64, None) == ab.ERR_VALUE
+    # C[9] is a float: sample indices beyond 2^24 are not representable
+    assert lib.arbor_setSample(A, -1, 0, None) == ab.ERR_VALUE
+    assert lib.arbor_setSample(A, (1 << 24) + 1, 0, None) == ab.ERR_VALUE
+    assert lib.arbor_setSample(None, 0, 1, None) == ab.ERR_NULL
 
 
 def test_image_sizes(lib):
@@ -111,3 +115,37 @@ def test_engine_rejections_without_device(lib):
 
 def test_launch_counter_starts_without_launches(lib):
     assert lib.arbor_launch_count() >= 0
+
+
+def test_batch_rejections_without_device(lib):
+    """Batch arguments are checked before any device work."""
+    import ctypes
+
+    import workloads
+
+    h = ctypes.c_void_p()
+    views = (ab.BatchView * 2)()
+    for v in views:
+        v.scene, v.width, v.height = 0, 64, 32
+        v.C[:] = [float(x) for x in workloads.view_pose_state(7, 64, 32, 0.0, 0.0, 0.0, 0.0)]
+    seeds = (ctypes.c_int * 2)(7, 1788)
+    assert lib.arbor_batch_create(None, seeds, 2, views, 2, None) == ab.ERR_NULL
+    assert lib.arbor_batch_create(ctypes.byref(h), seeds, 2, views, 0, None) == ab.ERR_VALUE
+    assert lib.arbor_batch_create(ctypes.byref(h), seeds, 0, views, 2, None) == ab.ERR_VALUE
+    bad_seeds = (ctypes.c_int * 2)(7, 1000001)
+    assert lib.arbor_batch_create(ctypes.byref(h), bad_seeds, 2, views, 2, None) == ab.ERR_VALUE
+    views[1].scene = 2
+    assert lib.arbor_batch_create(ctypes.byref(h), seeds, 2, views, 2, None) == ab.ERR_VALUE
+    assert b"scene 2" in lib.arbor_last_error()
+    views[1].scene, views[1].width = 1, 0
+    assert lib.arbor_batch_create(ctypes.byref(h), seeds, 2, views, 2, None) == ab.ERR_VALUE
+    views[1].width = 64
+    views[1].C[5] = float("nan")
+    assert lib.arbor_batch_create(ctypes.byref(h), seeds, 2, views, 2, None) == ab.ERR_VALUE
+    views[1].C[5] = 0.0
+    views[1].width = 65536 * 8 + 1
+    assert lib.arbor_batch_create(ctypes.byref(h), seeds, 2, views, 2, None) == ab.ERR_LIMIT
+    views[1].width = 64
+    assert lib.arbor_batch_create(ctypes.byref(h), seeds, 2, views, 2, None) == ab.ERR_NO_DEVICE
+    assert lib.arbor_batch_render(None) == ab.ERR_NULL
+    assert lib.arbor_batch_destroy(None) == ab.OK

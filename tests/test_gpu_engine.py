@@ -1,7 +1,6 @@
 """The C++ engine (src/engine.js restated) on the GPU: the host contract the
 reference tests with a fake device (tests/source.test.mjs:6) and the real-GPU
 checks of tests/browser.js:5-13."""
-import ctypes
 import zlib
 
 import numpy as np
@@ -9,40 +8,9 @@ import pytest
 import torch
 
 import arbor_b200 as ab
+from gpu_util import dev_array
 
 pytestmark = pytest.mark.gpu
-
-
-_RT = None
-
-
-def _cudart():
-    """The CUDA runtime torch itself loaded (used only to copy engine buffers out)."""
-    global _RT
-    if _RT is None:
-        import glob
-        import os
-
-        base = os.path.join(os.path.dirname(torch.__file__), "..", "nvidia")
-        cands = sorted(glob.glob(os.path.join(base, "cuda_runtime", "lib", "libcudart.so*")))
-        cands += ["libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so"]
-        for c in cands:
-            try:
-                _RT = ctypes.CDLL(c)
-                break
-            except OSError:
-                continue
-        _RT.cudaMemcpy.restype = ctypes.c_int
-        _RT.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
-    return _RT
-
-
-def dev_array(ptr: int, n: int, dtype=np.float32) -> np.ndarray:
-    """Copy n 4-byte elements at an engine device address to the host."""
-    torch.cuda.synchronize()
-    out = np.empty(n, dtype)
-    assert _cudart().cudaMemcpy(out.ctypes.data, ptr, n * 4, 2) == 0  # cudaMemcpyDeviceToHost
-    return out
 
 
 def fingerprint(a: np.ndarray) -> int:

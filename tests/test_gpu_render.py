@@ -227,3 +227,75 @@ def test_full_hd_frame_properties(cuda, oracle, scenes, gu, forest):
     xy = np.stack([idx % w, idx // w], 1).astype(np.int32)
     want = oracle.trace_pixel_list(scenes(1788), C, w, h, xy).reshape(-1, 4)[idx]
     assert np.mean(hits[idx, 1] == want[:, 1]) >= 0.995
+
+
+def test_progressive_wind_shadows_4spp(cuda, oracle, scenes, gu):
+    """The 4-spp frame with wind and sun shadows: samples 0..3 set through
+    arbor_setSample (C[9] = sample, C[10] = 1 on sample 0, as the harness's
+    render loop writes them, tests/native_harness.cpp:62) accumulate into
+    History; the accumulated image matches the oracle's."""
+    import workloads
+
+    w, h = 160, 96
+    s = scenes(7)
+    scene = gu.DevScene(s)
+    C = oracle.init_camera(s["P"], 7)
+    C[32], C[33] = w, h
+    C[22] = 1.0
+    C[12], C[13] = workloads.shadow_sun(7)
+    C[11], C[8] = 0.60, 0.75  # breeze on, 0.75 s into the animation
+    dC = gu.dev(C)
+    hit, lin, gui, fil = (gu.zeros_f(w * h * 4) for _ in range(4))
+    hist, px = gu.zeros_f(w * h * 4), gu.zeros_u(w * h)
+    hist_ref = np.zeros(w * h * 4, np.float32)
+    for sample in range(4):
+        gu.ok(cuda.call("arbor_setSample", dC, sample, int(sample == 0)))
+        assert gu.host(dC)[9] == sample and gu.host(dC)[10] == float(sample == 0)
+        gu.ok(cuda.call("arbor_tracePixels", scene.P, scene.Nodes, scene.Order, dC, hit, w, h))
+        gu.ok(cuda.call("arbor_shadePixels", scene.P, scene.Nodes, scene.Order, dC, hit, lin, gui, w, h))
+        gu.ok(cuda.call("arbor_filterResolve", lin, gui, hit, fil, hist, px, dC, w, h))
+        Cs = C.copy()
+        Cs[9], Cs[10] = sample, float(sample == 0)
+        ref = oracle.frame(s, Cs, w, h, History=hist_ref)
+        compare_hits(gu.host(hit), ref["Hit"], f"wind sample {sample}")
+    H, Hr = gu.host(hist).reshape(-1, 4), hist_ref.reshape(-1, 4)
+    assert (H[:, 3] == 4.0).all() and (Hr[:, 3] == 4.0).all()
+    err = np.max(np.abs(H[:, :3] - Hr[:, :3]) / np.maximum(1.0, np.abs(Hr[:, :3])), 1)
+    frac = float(np.mean(err <= 2e-3))
+    got, want = gu.host(px, np.uint32), ref["Pixels"]
+    lsb = np.max(np.abs(np.stack([(got >> k) & 255 for k in (0, 8, 16, 24)]).astype(int)
+                        - np.stack([(want >> k) & 255 for k in (0, 8, 16, 24)]).astype(int)), 0)
+    print(f"[4 spp wind shadows] History within 2e-3 on {frac:.5f}; Pixels within 1 LSB on {np.mean(lsb <= 1):.5f}")
+    assert frac >= 0.99
+    assert np.mean(lsb <= 1) >= 0.99
+
+
+def test_resolve_bytes_match_double_precision_gamma(cuda, gu):
+    """resolvePixels' bytes on a 1920x1080 frame of random radiance equal
+    those of the float of the double-precision pow(c, 1/2.2) (the kernel
+    takes a single-precision pow and falls back to the double one near byte
+    boundaries), computed here in numpy with the reference's float32
+    operations (Arbor.cu:303-304, packRGB :49)."""
+    w, h = 1920, 1080
+    rng = np.random.default_rng(5)
+    filt = (rng.random(w * h * 4, dtype=np.float32) * 3.0).astype(np.float32)
+    filt[::997] = 0.0
+    C = np.zeros(64, np.float32)
+    C[9], C[10], C[20] = 0.0, 1.0, 1.18
+    hist, px = gu.zeros_f(w * h * 4), gu.zeros_u(w * h)
+    gu.ok(cuda.call("arbor_resolvePixels", gu.dev(filt), hist, px, gu.dev(C), w, h))
+    got = gu.host(px, np.uint32)
+    f = np.float32
+    col = filt.reshape(-1, 4)[:, :3] * C[20]
+    ac = np.clip((col * (f(2.51) * col + f(0.03))) / (col * (f(2.43) * col + f(0.59)) + f(0.14)), f(0), f(1)).astype(np.float32)
+    g = np.power(ac.astype(np.float64), np.float64(f(1.0) / f(2.2))).astype(np.float32)
+    xs = np.tile(np.arange(w, dtype=np.float32), h)
+    ys = np.repeat(np.arange(h, dtype=np.float32), w)
+    u = (xs / f(w) - f(0.5)) * f(2.0)
+    v = (ys / f(h) - f(0.5)) * f(2.0)
+    vig = (f(1.0) - f(0.09) * (u * u + v * v)).astype(np.float32)
+    t = (np.clip(g * vig[:, None], f(0), f(1)) * f(255.0) + f(0.5)).astype(np.float32)
+    b = t.astype(np.uint32)
+    want = b[:, 0] | (b[:, 1] << 8) | (b[:, 2] << 16) | np.uint32(0xFF000000)
+    print(f"[gamma bytes] {np.count_nonzero(got != want)} of {w * h} pixels differ")
+    assert np.array_equal(got, want)
