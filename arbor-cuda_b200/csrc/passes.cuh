@@ -20,9 +20,18 @@ __device__ __forceinline__ void tile_pixel_at(int t, int x0, int y0, int tw, int
 // One ray per thread over 16x16-pixel CTAs (8x4-pixel warps); each warp's
 // primitive tests run warp-batched (warpbatch.cuh).
 struct PrimaryPolicy {
+  static constexpr int kRefill = 8;  // idle lanes that trigger a refill (measured best of 1-16)
   const Camera* cam;
   float* Hit;
   int width, height, pixel;
+  // The primary ray of pixel (x, y) with the ground plane as its initial
+  // nearest hit (tracePixels, Arbor.cu:252).
+  __device__ __forceinline__ void start(const TraceCtx& c, Ray& r, int x, int y) {
+    pixel = y * width + x;
+    f3 rd = camera_ray(*cam, x, y, width, height);
+    float ground = rd.y < -0.00001f ? -cam->ro.y / rd.y : kFar;
+    ray_begin(c, r, cam->ro, rd, ground > 0.0f ? ground : kFar);
+  }
   __device__ __forceinline__ void done(Ray& r) {
     reinterpret_cast<float4*>(Hit)[pixel] = make_float4(r.best, r.found, (float)r.foundTree, cam->c14 * r.best / (float)height);
     r.phase = kPhIdle;
@@ -38,12 +47,16 @@ __device__ __forceinline__ void trace_tile(const TraceCtx& c, const Camera& cam,
   PrimaryPolicy policy{&cam, Hit, width, height, y * width + x};
   Ray r;
   r.phase = kPhIdle;
-  if (x < width && y < height) {
-    f3 rd = camera_ray(cam, x, y, width, height);
-    float ground = rd.y < -0.00001f ? -cam.ro.y / rd.y : kFar;  // Arbor.cu:252
-    ray_begin(c, r, cam.ro, rd, ground > 0.0f ? ground : kFar);
-  }
+  if (x < width && y < height) policy.start(c, r, x, y);
   batch_run(c, r, b, policy);
+}
+
+// Primary rays of every pixel of a persistent CTA's pool.
+template <class WB>
+__device__ __forceinline__ void trace_pool(const TraceCtx& c, const Camera& cam, WB& b, float* __restrict__ Hit, const PixelPool& pool) {
+  PrimaryPolicy policy{&cam, Hit, pool.width, pool.height, 0};
+  Ray r;
+  batch_run_pool(c, r, b, policy, pool);
 }
 
 // ---------------------------------------------------------------- shade --
@@ -318,9 +331,27 @@ struct ShadePolicy {
   float* Linear;
   float* Guide;
   const TraceCtx* ctx;
+  const Camera* cam;
+  const Instance* inst;
+  const float* Hit;
+  int width, height;
   int pixel, seg;
   f3 trans;
   Shading sh;
+  // Shade pixel (x, y): the surface terms, then the first shadow segment
+  // toward the sun, or the final colour when no visibility is needed.
+  __device__ __forceinline__ void start(const TraceCtx& c, Ray& r, int x, int y) {
+    pixel = y * width + x;
+    shade_pre<kForestScene>(P, *cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + pixel), x, y, width, height, sh);
+    if (!sh.final && sh.shadow) {
+      trans = mk(1.0f, 1.0f, 1.0f);
+      seg = 0;
+      ray_begin(c, r, sh.origin, sh.light, 36.0f);
+    } else {
+      write(mk(1.0f, 1.0f, 1.0f));
+      r.phase = kPhIdle;
+    }
+  }
   __device__ __forceinline__ void write(f3 visibility) {
     f3 col = shade_post(sh, visibility);
     reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
@@ -357,19 +388,14 @@ __device__ __forceinline__ void shade_tile(const TraceCtx& c, const Camera& cam,
   policy.Linear = Linear;
   policy.Guide = Guide;
   policy.ctx = &c;
-  policy.pixel = y * width + x;
+  policy.cam = &cam;
+  policy.inst = inst;
+  policy.Hit = Hit;
+  policy.width = width;
+  policy.height = height;
   Ray r;
   r.phase = kPhIdle;
-  if (x < width && y < height) {
-    shade_pre<kForestScene>(P, cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + policy.pixel), x, y, width, height, policy.sh);
-    if (!policy.sh.final && policy.sh.shadow) {
-      policy.trans = mk(1.0f, 1.0f, 1.0f);
-      policy.seg = 0;
-      ray_begin(c, r, policy.sh.origin, policy.sh.light, 36.0f);
-    } else {
-      policy.write(mk(1.0f, 1.0f, 1.0f));
-    }
-  }
+  if (x < width && y < height) policy.start(c, r, x, y);
   batch_run(c, r, b, policy);
 }
 

@@ -2,11 +2,14 @@
 // filterLighting, resolvePixels (Arbor.cu:252-304) and their single-tree and
 // fused variants, with their C-ABI entry points.
 //
-// Launch shape: 256-thread blocks over 16x16 pixel tiles, each warp an 8x4
-// sub-tile so neighbouring rays share traversal paths.  Each trace/shade
-// block builds the 324-entry forest instance table in shared memory once;
-// every table entry equals what the reference's forest helpers recompute per
-// ray (Arbor.cu:57-69).
+// Launch shapes: the trace is persistent (2 CTAs per SM, lanes taking pixels
+// of 8x4 blocks as their rays finish); the shade runs 256-thread blocks over
+// 16x16 pixel tiles, each warp an 8x4 sub-tile so neighbouring rays share
+// traversal paths.  Each trace/shade block builds the 324-entry forest
+// instance table in shared memory once; every table entry equals what the
+// reference's forest helpers recompute per ray (Arbor.cu:57-69).
+#include <algorithm>
+
 #include "abi_util.h"
 #include "passes.cuh"
 
@@ -14,21 +17,8 @@ namespace arbor {
 namespace {
 
 // ---------------------------------------------------------------- kernels --
-// One ray per thread over 16x16-pixel CTAs (8x4-pixel warps); each warp's
-// primitive tests run warp-batched (warpbatch.cuh).
-template <bool kForestScene>
-__global__ void __launch_bounds__(kBlock, 2) trace_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
-                                                          const uint32_t* __restrict__ Order, const float* __restrict__ C,
-                                                          float* __restrict__ Hit, int width, int height) {
-  extern __shared__ float4 batch_smem[];
-  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
-  __shared__ Camera cam;
-  __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
-  const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, kForestScene};
-  trace_tile(c, cam, b, Hit, width, height, blockIdx.x * kTile, blockIdx.y * kTile, kTile);
-}
-
+// Shading: one pixel per thread over 16x16-pixel CTAs (8x4-pixel warps);
+// each warp's shadow-ray primitive tests run warp-batched (warpbatch.cuh).
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock, 2) shade_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                           const uint32_t* __restrict__ Order, const float* __restrict__ C,
@@ -41,6 +31,26 @@ __global__ void __launch_bounds__(kBlock, 2) shade_kernel(const float* __restric
   block_setup(C, cam, inst, kForestScene);
   const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
   shade_tile<kForestScene>(c, cam, inst, b, P, Hit, Linear, Guide, width, height, blockIdx.x * kTile, blockIdx.y * kTile, kTile);
+}
+
+// Persistent form of the trace: a grid of (SMs x 2) CTAs, each taking every
+// gridDim.x-th 8x4-pixel block of the image, its lanes taking pixels as
+// their rays finish (batch_run_pool).
+template <bool kForestScene>
+__global__ void __launch_bounds__(kBlock, 2) trace_pool_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                               const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                               float* __restrict__ Hit, int width, int height) {
+  extern __shared__ float4 batch_smem[];
+  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForestScene ? kForest : 1];
+  __shared__ int next;
+  if (threadIdx.x == 0) next = 0;
+  block_setup(C, cam, inst, kForestScene);
+  const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, kForestScene};
+  const int bx = (width + 7) / 8;
+  const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
+  trace_pool(c, cam, b, Hit, pool);
 }
 
 template <bool kResolve>
@@ -83,6 +93,17 @@ inline bool batch_smem_ready(const void* kernel) {
 }
 
 dim3 pixel_grid(int w, int h) { return dim3((w + kTile - 1) / kTile, (h + kTile - 1) / kTile); }
+
+// Persistent grid: 2 CTAs per SM (the register and shared-memory limit of
+// the batched tracer), or one CTA per 8x4 block when the image has fewer.
+dim3 pool_grid(int w, int h) {
+  static int sms[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  if (sms[dev] == 0 && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms[dev] = 148;
+  const long blocks = (long)((w + 7) / 8) * ((h + 3) / 4);
+  return dim3((unsigned)std::min<long>(blocks, 2L * sms[dev]));
+}
 dim3 filter_grid(int w, int h) { return dim3((w + kFX - 1) / kFX, (h + kFY - 1) / kFY); }
 
 int trace_entry(const char* name, bool forest, const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width,
@@ -96,14 +117,14 @@ int trace_entry(const char* name, bool forest, const float* P, const float* Node
                        {Hit, empty ? 0 : image_bytes(width, height), true, 16, "Hit"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
-  if (!batch_smem_ready(forest ? (const void*)trace_kernel<true> : (const void*)trace_kernel<false>)) {
+  if (!batch_smem_ready(forest ? (const void*)trace_pool_kernel<true> : (const void*)trace_pool_kernel<false>)) {
     set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
     return ARBOR_ERR_CUDA;
   }
   if (forest)
-    trace_kernel<true><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
   else
-    trace_kernel<false><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
   count_launch();
   return check_launch(name);
 }
@@ -122,6 +143,9 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
     set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
     return ARBOR_ERR_CUDA;
   }
+  // Shading stays on fixed tiles: its per-pixel start (surface terms,
+  // normals) is long, and refilling lanes one by one ran it with few lanes
+  // active (measured slower than tiles).
   if (forest)
     shade_kernel<true><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
   else

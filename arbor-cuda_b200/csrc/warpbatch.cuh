@@ -233,4 +233,79 @@ __device__ __forceinline__ void batch_run(const TraceCtx& c, Ray& r, WB& b, Poli
   }
 }
 
+// The pixels of a persistent CTA: the 8x4-pixel blocks blockIdx.x,
+// blockIdx.x + gridDim.x, blockIdx.x + 2 gridDim.x, ... of a width x height
+// image, handed out one pixel at a time, in block order, from a counter in
+// shared memory.
+struct PixelPool {
+  int* next;  // shared-memory counter of pixels handed out by this CTA
+  int width, height, blocks_x, blocks;
+};
+
+// Collective (all 32 lanes): hand the next pixels to the lanes in `idle`.
+// Returns true for a lane that received a pixel inside the image; `past` is
+// set for every lane once the CTA's blocks are used up.
+__device__ __forceinline__ bool pool_take(const PixelPool& pool, unsigned idle, int lane, int& x, int& y, bool& past) {
+  const unsigned full = 0xffffffffu;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(pool.next, __popc(idle));
+  base = __shfl_sync(full, base, 0);
+  bool got = false, beyond = false;
+  if (idle & (1u << lane)) {
+    const int idx = base + __popc(idle & ((1u << lane) - 1u));
+    const int block = (int)blockIdx.x + (idx >> 5) * (int)gridDim.x;
+    if (block >= pool.blocks) {
+      beyond = true;
+    } else {
+      const int by = block / pool.blocks_x, bx = block - by * pool.blocks_x;
+      x = bx * 8 + (idx & 7);
+      y = by * 4 + ((idx >> 3) & 3);
+      got = x < pool.width && y < pool.height;
+    }
+  }
+  past = __any_sync(full, beyond);
+  return got;
+}
+
+// Drive one warp through a pixel pool: lanes whose rays are finished take
+// the next pixels (Policy::start begins a ray, or finishes the pixel at
+// once), so no lane waits for the slowest ray of a fixed tile.  Policy::done
+// is called for a finished ray and either continues it (a new trace on r) or
+// sets it idle.
+template <class WB, class Policy>
+__device__ __forceinline__ void batch_run_pool(const TraceCtx& c, Ray& r, WB& b, Policy& policy, const PixelPool& pool) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int nq = 0;
+  bool drained = false;
+  r.phase = kPhIdle;
+  for (;;) {
+    if (!drained) {
+      const unsigned idle = __ballot_sync(full, r.phase == kPhIdle);
+      // Refill once Policy::kRefill lanes are idle (or all are): a policy
+      // whose start is long (shading) runs it with more lanes together.
+      if (idle && (__popc(idle) >= Policy::kRefill || idle == full)) {
+        int x = 0, y = 0;
+        bool past = false;
+        const bool got = pool_take(pool, idle, lane, x, y, past);
+        drained = past;
+        if (got) policy.start(c, r, x, y);
+      }
+    }
+    for (;;) {
+      batch_advance(c, r, b, lane, nq);
+      if (r.phase != kPhDone) break;
+      policy.done(r);
+    }
+    const bool pending = nq > 0;
+    if (!__any_sync(full, pending)) {
+      // every lane is idle: take more pixels, or stop when none are left
+      if (drained) break;
+      continue;
+    }
+    batch_tests(c, r, b, lane, nq);
+    batch_apply(c, r, b, lane, nq);
+  }
+}
+
 }  // namespace arbor
