@@ -89,6 +89,7 @@ SIGNATURES = {
     "arbor_buildScene": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "arbor_traceTreePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_shadeTreePixels": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
+    "arbor_shadeGBuffer": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_filterResolve": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_trace_work_slots": (ctypes.c_size_t, [_i, _i]),
     "arbor_traceWork": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
@@ -116,6 +117,17 @@ SIGNATURES = {
     "arbor_batch_inspect": (_i, [_vp, ctypes.POINTER(BatchInfo)]),
     "arbor_batch_read_pixels": (_i, [_vp, _vp, ctypes.c_size_t]),
     "arbor_batch_destroy": (_i, [_vp]),
+    "arbor_denoiser_create": (_i, [ctypes.POINTER(_vp), _i, _i, _i, ctypes.c_uint32, _vp]),
+    "arbor_denoiser_param_count": (_i, [_vp, ctypes.POINTER(ctypes.c_size_t)]),
+    "arbor_denoiser_get_params": (_i, [_vp, _vp, ctypes.c_size_t]),
+    "arbor_denoiser_set_params": (_i, [_vp, _vp, ctypes.c_size_t]),
+    "arbor_denoiser_features": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "arbor_denoiser_train_step": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _f, ctypes.POINTER(_f)]),
+    "arbor_denoiser_infer": (_i, [_vp, _vp, _vp, _vp, _i, _i]),
+    "arbor_denoiser_set_backend": (_i, [_vp, _i]),
+    "arbor_denoiser_check": (_i, [_vp]),
+    "arbor_denoiser_destroy": (_i, [_vp]),
+    "arbor_accumulate": (_i, [_vp, _vp, ctypes.c_size_t, _f, _vp]),
 }
 
 

@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libarbor_b200.so")
-SOURCES = ["build.cu", "camera.cu", "render.cu", "count.cu", "engine.cu", "batch.cu"]
+SOURCES = ["build.cu", "camera.cu", "render.cu", "count.cu", "engine.cu", "batch.cu", "denoise.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",

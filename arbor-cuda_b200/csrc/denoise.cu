@@ -1,0 +1,1195 @@
+// denoise.cu - the learned denoiser: a 4-level convolutional encoder-decoder
+// (U-Net, channels 32/64/96/128, 3x3 kernels) over the 1-spp radiance and
+// the albedo / normal / depth G-buffer, trained and run on the GPU by the
+// kernels in this file.  No reference counterpart: the reference's only
+// denoiser is filterLighting (Arbor.cu:292-302), which stays available.
+//
+// Arithmetic: activations and weights in BF16, tensor-core products
+// accumulated in FP32 (tcgen05.mma with TMEM accumulators for the forward
+// convolutions; mma.sync m16n8k16 for the backward passes), FP32 master
+// weights, biases, gradients and Adam moments.  Activations are NHWC with channel counts that
+// are multiples of 16.
+//
+// Kernels:
+//   conv_tc_kernel  the forward 3x3 convolutions on tcgen05 (TMEM
+//                   accumulators), used by inference and training
+//   conv_kernel     3x3 convolution as an implicit GEMM: a CTA computes an
+//                   8x8-pixel tile (partial at the image edge) for 16, 32 or
+//                   64 output channels; input halo
+//                   and weights are staged in shared memory 16 or 32 input
+//                   channels at a time.  The same kernel runs the backward
+//                   data pass on rotated, transposed weights, with the
+//                   previous layer's activation derivative in its epilogue.
+//   wgrad_kernel    weight gradients: a GEMM over pixels of the output
+//                   gradient and the shifted input, FP32 atomics per CTA
+//   pool / upcat    2x2 average pooling, nearest upsampling + skip concat,
+//                   and their backward passes with activation derivatives
+//   loss, adam, features, output: elementwise
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "abi_util.h"
+#include "arbor_math.cuh"
+
+namespace arbor {
+namespace {
+
+typedef __nv_bfloat16 bf16;
+constexpr float kSlope = 0.1f;  // leaky ReLU
+constexpr int kFeat = 16;       // input feature channels (13 used)
+constexpr int kOutC = 16;       // output channels (3 used)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n" : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n" : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(addr));
+}
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// ------------------------------------------------------------ convolution --
+struct ConvArgs {
+  const bf16* x;      // input NHWC, cin channels
+  const bf16* wt;     // weights [cout][9][cin]
+  const float* bias;  // nullable
+  void* y;            // output NHWC, cout channels (bf16, or fp32 when y_fp32)
+  const bf16* mask;   // nullable: multiply by the leaky-ReLU derivative at mask (NHWC, cout channels)
+  int cin, cout, n, h, w;
+  int act;            // leaky ReLU on the output
+  int y_fp32;
+};
+
+// smem layout of one stage: halo [100][KC+8], weights [NT*8*9][KC+8] (bf16)
+template <int KC, int NT>
+constexpr int conv_smem_bytes() {
+  return (100 + NT * 8 * 9) * (KC + 8) * 2;
+}
+
+template <int KC, int NT>
+__global__ void __launch_bounds__(128) conv_kernel(ConvArgs a) {
+  extern __shared__ uint4 conv_smem[];
+  constexpr int RS = KC + 8;  // row stride (elements): 16-byte aligned rows, staggered banks
+  bf16* halo = reinterpret_cast<bf16*>(conv_smem);
+  bf16* wts = halo + 100 * RS;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles_x = (a.w + 7) >> 3;
+  const int ty = blockIdx.x / tiles_x, tx = blockIdx.x - ty * tiles_x;
+  const int co0 = blockIdx.y * NT * 8;
+  const int img = blockIdx.z;
+  float acc[NT][4];
+#pragma unroll
+  for (int i = 0; i < NT; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0f;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (int c0 = 0; c0 < a.cin; c0 += KC) {
+    // input halo: 10x10 pixels x KC channels, zero outside the image
+    for (int v = tid; v < 100 * (KC / 8); v += 128) {
+      const int pix = v / (KC / 8), part = v - pix * (KC / 8);
+      const int hy = pix / 10, hx = pix - hy * 10;
+      const int gy = ty * 8 + hy - 1, gx = tx * 8 + hx - 1;
+      uint4 val = zero;
+      if (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w)
+        val = *reinterpret_cast<const uint4*>(a.x + ((size_t)(img * a.h + gy) * a.w + gx) * a.cin + c0 + part * 8);
+      *reinterpret_cast<uint4*>(halo + pix * RS + part * 8) = val;
+    }
+    // weights: NT*8 output channels x 9 taps x KC input channels
+    for (int v = tid; v < NT * 8 * 9 * (KC / 8); v += 128) {
+      const int row = v / (KC / 8), part = v - row * (KC / 8);
+      const int co = co0 + row / 9, tap = row - (row / 9) * 9;
+      uint4 val = zero;
+      if (co < a.cout) val = *reinterpret_cast<const uint4*>(a.wt + ((size_t)co * 9 + tap) * a.cin + c0 + part * 8);
+      *reinterpret_cast<uint4*>(wts + row * RS + part * 8) = val;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int tap = 0; tap < 9; tap++) {
+      const int dy = tap / 3, dx = tap - dy * 3;
+#pragma unroll
+      for (int kk = 0; kk < KC / 16; kk++) {
+        uint32_t a0, a1, a2, a3;
+        {
+          const int r = lane & 15, koff = (lane >> 4) * 8;
+          const int hp = (2 * warp + (r >> 3) + dy) * 10 + (r & 7) + dx;
+          ldsm_x4(smem_u32(halo + hp * RS + kk * 16 + koff), a0, a1, a2, a3);
+        }
+#pragma unroll
+        for (int nt = 0; nt < NT; nt += 2) {
+          const int mi = lane >> 3;
+          const int col = (nt + (mi >> 1)) * 8 + (lane & 7);
+          uint32_t b0, b1, b2, b3;
+          ldsm_x4(smem_u32(wts + (col * 9 + tap) * RS + kk * 16 + (mi & 1) * 8), b0, b1, b2, b3);
+          mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
+          mma_bf16(acc[nt + 1], a0, a1, a2, a3, b2, b3);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // epilogue: bias, activation or activation derivative, store
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; nt++) {
+    const int co = co0 + nt * 8 + 2 * t;
+    if (co >= a.cout) continue;
+    const float b0 = a.bias ? a.bias[co] : 0.0f, b1 = a.bias ? a.bias[co + 1] : 0.0f;
+#pragma unroll
+    for (int hh = 0; hh < 2; hh++) {
+      const int r = g + 8 * hh;
+      const int gy = ty * 8 + 2 * warp + (r >> 3), gx = tx * 8 + (r & 7);
+      if (gy >= a.h || gx >= a.w) continue;  // partial tile at the image edge
+      const size_t p = (size_t)(img * a.h + gy) * a.w + gx;
+      float v0 = acc[nt][2 * hh] + b0, v1 = acc[nt][2 * hh + 1] + b1;
+      if (a.act) {
+        v0 = v0 > 0.0f ? v0 : v0 * kSlope;
+        v1 = v1 > 0.0f ? v1 : v1 * kSlope;
+      }
+      if (a.mask) {
+        const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162*>(a.mask + p * a.cout + co);
+        if (!(__bfloat162float(m.x) > 0.0f)) v0 *= kSlope;
+        if (!(__bfloat162float(m.y) > 0.0f)) v1 *= kSlope;
+      }
+      if (a.y_fp32)
+        *reinterpret_cast<float2*>(reinterpret_cast<float*>(a.y) + p * a.cout + co) = make_float2(v0, v1);
+      else
+        *reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<bf16*>(a.y) + p * a.cout + co) = __floats2bfloat162_rn(v0, v1);
+    }
+  }
+}
+
+// ------------------------------------------- tcgen05 convolution (sm_100a) --
+// The same 3x3 convolution on the 5th-generation tensor cores: a CTA of 4
+// warps computes 128 consecutive pixels of one output row for all N output
+// channels.  Per chunk of CC input channels it stages the 3 input rows
+// (130 pixels with the halo) and the chunk's weights in shared memory, in the
+// K-major, non-swizzled core-matrix layout the MMA reads (8 rows of 16 bytes
+// per core matrix): a tap's A operand is the staged rows shifted by the tap,
+// so one 128-row descriptor per tap needs no copy.  One thread issues
+// tcgen05.mma (M = 128, N, K = 16, BF16 inputs, FP32 accumulator in TMEM)
+// for 9 taps x CC/16 steps, commits to an mbarrier, and every thread waits
+// (bounded) before the next chunk overwrites the operands.  The epilogue reads
+// the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 =
+// pixels 32w..32w+31 of the tile), applies bias and activation and stores
+// BF16 or FP32.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  // start address, leading / stride byte offsets (16-byte units), version 1,
+  // no swizzle (layout type 0)
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+         (1ull << 46);
+}
+template <int N>
+constexpr uint32_t umma_idesc() {
+  // FP32 accumulator, BF16 A and B, both K-major, N >> 3, M = 128 >> 4
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+template <int N>
+constexpr int tmem_cols() {
+  return N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+}
+template <int N, int CC>
+constexpr int conv_tc_smem_bytes() {
+  return (CC / 8) * 3 * 130 * 16 + 9 * (CC / 8) * N * 16 + 16;
+}
+
+// Bounded wait on an mbarrier phase; false when it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (int i = 0; i < (1 << 20); i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int N, int CC>
+__global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
+  extern __shared__ __align__(128) uint8_t tc_smem[];
+  constexpr int KU = CC / 8;               // 16-byte K units per chunk
+  constexpr int HALO_B = KU * 3 * 130 * 16;
+  constexpr int W_B = 9 * KU * N * 16;
+  constexpr uint32_t LBO_A = 3 * 130 * 16;  // next K unit of the halo
+  constexpr uint32_t LBO_B = N * 16;        // next K unit of the weights
+  constexpr int COLS = tmem_cols<N>();
+  uint8_t* halo = tc_smem;
+  uint8_t* wts = tc_smem + HALO_B;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + HALO_B + W_B);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles_x = (a.w + 127) >> 7;
+  int t = blockIdx.x;
+  const int tx = t % tiles_x;
+  t /= tiles_x;
+  const int y = t % a.h, img = t / a.h;
+  const int x0 = tx * 128;
+  const uint32_t bar_a = smem_u32(bar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)), "r"(COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_a), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int c0 = 0; c0 < a.cin && ok; c0 += CC) {
+    // input rows y-1..y+1, pixels x0-1..x0+128, CC channels: unit (k, r, hx)
+    for (int v = tid; v < 3 * 130 * KU; v += 128) {
+      const int k = v % KU, rh = v / KU;
+      const int r = rh / 130, hx = rh - r * 130;
+      const int gy = y + r - 1, gx = x0 + hx - 1;
+      uint4 val = zero;
+      if (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w)
+        val = *reinterpret_cast<const uint4*>(a.x + ((size_t)(img * a.h + gy) * a.w + gx) * a.cin + c0 + k * 8);
+      *reinterpret_cast<uint4*>(halo + ((k * 3 + r) * 130 + hx) * 16) = val;
+    }
+    // weights: unit (tap, k, n)
+    for (int v = tid; v < 9 * KU * N; v += 128) {
+      const int k = v % KU, q = v / KU;
+      const int tap = q % 9, n = q / 9;
+      uint4 val = zero;
+      if (n < a.cout) val = *reinterpret_cast<const uint4*>(a.wt + ((size_t)n * 9 + tap) * a.cin + c0 + k * 8);
+      *reinterpret_cast<uint4*>(wts + ((tap * KU + k) * N + n) * 16) = val;
+    }
+    // make the generic-proxy stores visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t idesc = umma_idesc<N>();
+#pragma unroll 1
+      for (int tap = 0; tap < 9; tap++) {
+        const int dy = tap / 3, dx = tap - dy * 3;
+#pragma unroll
+        for (int st = 0; st < CC / 16; st++) {
+          const uint64_t da = umma_desc(smem_u32(halo + ((2 * st * 3 + dy) * 130 + dx) * 16), LBO_A, 128);
+          const uint64_t db = umma_desc(smem_u32(wts + ((tap * KU + 2 * st) * N) * 16), LBO_B, 128);
+          const uint32_t acc = (c0 > 0 || tap > 0 || st > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+              "l"(da), "l"(db), "r"(idesc), "r"(acc));
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_a) : "memory");
+    }
+    // every thread waits for the MMAs (bounded); the barrier makes the
+    // outcome uniform, so all threads leave the loop together
+    ok = __syncthreads_and(mbar_wait(bar_a, phase) ? 1 : 0) != 0;
+    phase ^= 1u;
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const int r = warp * 32 + lane;  // this thread's TMEM lane = pixel of the tile
+    const int gx = x0 + r;
+    const size_t p = (size_t)(img * a.h + y) * a.w + gx;
+#pragma unroll 1
+    for (int col = 0; col < N; col += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]),
+            "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (gx < a.w) {
+        float f[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int co = col + j;
+          float x = __uint_as_float(v[j]) + (a.bias ? a.bias[co] : 0.0f);
+          if (a.act) x = x > 0.0f ? x : x * kSlope;
+          if (a.mask && !(__bfloat162float(a.mask[p * a.cout + co]) > 0.0f)) x *= kSlope;
+          f[j] = x;
+        }
+        if (a.y_fp32) {
+          float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(a.y) + p * a.cout + col);
+#pragma unroll
+          for (int j = 0; j < 4; j++) o[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+        } else {
+          uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(a.y) + p * a.cout + col);
+          uint32_t w[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+            w[j] = *reinterpret_cast<const uint32_t*>(&b2);
+          }
+          o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+          o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(COLS));
+}
+
+// ------------------------------------------------------- weight gradient --
+// dW[co][tap][ci] += sum over pixels p of dY[p][co] * X[p + tap offset][ci].
+// CTA: 64 output channels (4 warps x 16) x CI (16 or 32) input channels of
+// one tap, over a contiguous range of pixels, 32 at a time.
+struct WgradArgs {
+  const bf16* dy;  // NHWC, cout channels
+  const bf16* x;   // NHWC, cin channels
+  float* dw;       // [cout][9][cin], accumulated
+  int cin, cout, n, h, w;
+  int pixels_per_cta;
+};
+
+template <int CI>
+__global__ void __launch_bounds__(128) wgrad_kernel(WgradArgs a) {
+  constexpr int KP = 32;   // pixels per stage
+  constexpr int NT = CI / 8;
+  constexpr int DS = 64 + 8, XS = CI + 8;
+  __shared__ __align__(16) bf16 dys[KP * DS];
+  __shared__ __align__(16) bf16 xs[KP * XS];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int co0 = blockIdx.y * 64;
+  const int chunks = a.cin / CI;
+  const int tap = blockIdx.z / chunks, ci0 = (blockIdx.z - tap * chunks) * CI;
+  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  const long total = (long)a.n * a.h * a.w;
+  const long p_begin = (long)blockIdx.x * a.pixels_per_cta;
+  const long p_end = p_begin + a.pixels_per_cta < total ? p_begin + a.pixels_per_cta : total;
+  float acc[NT][4];
+#pragma unroll
+  for (int i = 0; i < NT; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0f;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (long pb = p_begin; pb < p_end; pb += KP) {
+    // dY rows: KP pixels x 64 channels
+    for (int v = tid; v < KP * 8; v += 128) {
+      const int r = v >> 3, part = v & 7;
+      const long p = pb + r;
+      const int co = co0 + part * 8;
+      uint4 val = zero;
+      if (p < p_end && co < a.cout) val = *reinterpret_cast<const uint4*>(a.dy + p * a.cout + co);
+      *reinterpret_cast<uint4*>(dys + r * DS + part * 8) = val;
+    }
+    // shifted X rows: KP pixels x CI channels
+    for (int v = tid; v < KP * (CI / 8); v += 128) {
+      const int r = v / (CI / 8), part = v - r * (CI / 8);
+      const long p = pb + r;
+      uint4 val = zero;
+      if (p < p_end) {
+        const int img = (int)(p / ((long)a.h * a.w));
+        const int rem = (int)(p - (long)img * a.h * a.w);
+        const int y = rem / a.w + dy, xx = rem % a.w + dx;
+        if (y >= 0 && y < a.h && xx >= 0 && xx < a.w)
+          val = *reinterpret_cast<const uint4*>(a.x + ((size_t)(img * a.h + y) * a.w + xx) * a.cin + ci0 + part * 8);
+      }
+      *reinterpret_cast<uint4*>(xs + r * XS + part * 8) = val;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kb = 0; kb < KP; kb += 16) {
+      const int mi = lane >> 3, row = lane & 7;
+      uint32_t a0, a1, a2, a3;
+      // A[m = co][k = pixel] from dY rows (pixel-major): transposed loads
+      ldsm_x4_t(smem_u32(dys + (kb + (mi >> 1) * 8 + row) * DS + warp * 16 + (mi & 1) * 8), a0, a1, a2, a3);
+#pragma unroll
+      for (int nt = 0; nt < NT; nt += 2) {
+        uint32_t b0, b1, b2, b3;
+        ldsm_x4_t(smem_u32(xs + (kb + (mi & 1) * 8 + row) * XS + (nt + (mi >> 1)) * 8), b0, b1, b2, b3);
+        mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
+        mma_bf16(acc[nt + 1], a0, a1, a2, a3, b2, b3);
+      }
+    }
+    __syncthreads();
+  }
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; nt++) {
+#pragma unroll
+    for (int hh = 0; hh < 2; hh++) {
+      const int co = co0 + warp * 16 + g + 8 * hh;
+      if (co >= a.cout) continue;
+      const int ci = ci0 + nt * 8 + 2 * t;
+      float* d = a.dw + ((size_t)co * 9 + tap) * a.cin + ci;
+      atomicAdd(d, acc[nt][2 * hh]);
+      atomicAdd(d + 1, acc[nt][2 * hh + 1]);
+    }
+  }
+}
+
+// db[co] += sum over pixels of dY[p][co]
+__global__ void bgrad_kernel(const bf16* __restrict__ dy, float* __restrict__ db, int cout, long pixels) {
+  __shared__ float part[256];
+  const int tid = threadIdx.x;
+  const int lanes = 256 / cout * cout;  // threads that own a channel
+  float s = 0.0f;
+  if (tid < lanes) {
+    const int co = tid % cout;
+    for (long p = (long)blockIdx.x * (256 / cout) + tid / cout; p < pixels; p += (long)gridDim.x * (256 / cout))
+      s += __bfloat162float(dy[p * cout + co]);
+  }
+  part[tid] = s;
+  __syncthreads();
+  if (tid < cout) {
+    float t = 0.0f;
+    for (int k = tid; k < lanes; k += cout) t += part[k];
+    atomicAdd(db + tid, t);
+  }
+}
+
+// --------------------------------------------------- pooling and concat --
+__global__ void pool_kernel(const bf16* __restrict__ x, bf16* __restrict__ y, int n, int h, int w, int c) {
+  const long total = (long)n * (h / 2) * (w / 2) * c;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int ch = (int)(i % c);
+    long q = i / c;
+    const int X = (int)(q % (w / 2));
+    q /= (w / 2);
+    const int Y = (int)(q % (h / 2));
+    const int img = (int)(q / (h / 2));
+    const size_t b = ((size_t)(img * h + 2 * Y) * w + 2 * X) * c + ch;
+    const float s = __bfloat162float(x[b]) + __bfloat162float(x[b + c]) + __bfloat162float(x[b + (size_t)w * c]) +
+                    __bfloat162float(x[b + (size_t)w * c + c]);
+    y[i] = __float2bfloat16(0.25f * s);
+  }
+}
+
+// d(skip)[p] = (0.25 * d(pooled)[parent] + dcat[p]) * act'(skip[p])
+__global__ void pool_back_kernel(const bf16* __restrict__ dpool, const bf16* __restrict__ dcat, const bf16* __restrict__ skip,
+                                 bf16* __restrict__ dx, int n, int h, int w, int c) {
+  const long total = (long)n * h * w * c;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int ch = (int)(i % c);
+    long q = i / c;
+    const int x = (int)(q % w);
+    q /= w;
+    const int y = (int)(q % h);
+    const int img = (int)(q / h);
+    float g = 0.25f * __bfloat162float(dpool[((size_t)(img * (h / 2) + y / 2) * (w / 2) + x / 2) * c + ch]) + __bfloat162float(dcat[i]);
+    if (!(__bfloat162float(skip[i]) > 0.0f)) g *= kSlope;
+    dx[i] = __float2bfloat16(g);
+  }
+}
+
+// out[p] = concat(skip[p] (cs), low[parent(p)] (cl))
+__global__ void upcat_kernel(const bf16* __restrict__ skip, const bf16* __restrict__ low, bf16* __restrict__ out, int n, int h, int w, int cs,
+                             int cl) {
+  const int c = cs + cl;
+  const long total = (long)n * h * w * c;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int ch = (int)(i % c);
+    const long p = i / c;
+    if (ch < cs) {
+      out[i] = skip[p * cs + ch];
+    } else {
+      const int x = (int)(p % w);
+      const long q = p / w;
+      const int y = (int)(q % h);
+      const int img = (int)(q / h);
+      out[i] = low[((size_t)(img * (h / 2) + y / 2) * (w / 2) + x / 2) * cl + (ch - cs)];
+    }
+  }
+}
+
+// dcat -> d(skip part) unmasked (dskip), d(low)[q] = sum of its 4 children's gradients * act'(low[q])
+__global__ void upcat_back_kernel(const bf16* __restrict__ dcat, const bf16* __restrict__ low, bf16* __restrict__ dskip,
+                                  bf16* __restrict__ dlow, int n, int h, int w, int cs, int cl) {
+  const int c = cs + cl;
+  const long skip_total = (long)n * h * w * cs;
+  const long low_total = (long)n * (h / 2) * (w / 2) * cl;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < skip_total + low_total; i += (long)gridDim.x * blockDim.x) {
+    if (i < skip_total) {
+      const long p = i / cs;
+      dskip[i] = dcat[p * c + (i - p * cs)];
+    } else {
+      const long j = i - skip_total;
+      const int ch = (int)(j % cl);
+      long q = j / cl;
+      const int X = (int)(q % (w / 2));
+      q /= (w / 2);
+      const int Y = (int)(q % (h / 2));
+      const int img = (int)(q / (h / 2));
+      const size_t b = ((size_t)(img * h + 2 * Y) * w + 2 * X) * c + cs + ch;
+      float g = __bfloat162float(dcat[b]) + __bfloat162float(dcat[b + c]) + __bfloat162float(dcat[b + (size_t)w * c]) +
+                __bfloat162float(dcat[b + (size_t)w * c + c]);
+      if (!(__bfloat162float(low[j]) > 0.0f)) g *= kSlope;
+      dlow[j] = __float2bfloat16(g);
+    }
+  }
+}
+
+// ----------------------------------------------------------- elementwise --
+// Features of one pixel: log(1 + radiance), albedo, normal,
+// log(1 + depth) / 4, log(1 + filterLighting's radiance).
+__global__ void features_kernel(const float4* __restrict__ lin, const float4* __restrict__ gui, const float4* __restrict__ nrm,
+                                const float4* __restrict__ hit, const float4* __restrict__ fil, bf16* __restrict__ f, long pixels) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += (long)gridDim.x * blockDim.x) {
+    const float4 l = lin[p], g = gui[p], n = nrm[p], h = hit[p], q = fil[p];
+    const float depth = fminf(fmaxf(h.x, 0.0f), 1.0e4f);
+    float v[kFeat] = {log1pf(fmaxf(l.x, 0.0f)), log1pf(fmaxf(l.y, 0.0f)), log1pf(fmaxf(l.z, 0.0f)), g.x, g.y, g.z, n.x, n.y, n.z,
+                      log1pf(depth) * 0.25f, log1pf(fmaxf(q.x, 0.0f)), log1pf(fmaxf(q.y, 0.0f)), log1pf(fmaxf(q.z, 0.0f)),
+                      0.0f, 0.0f, 0.0f};
+    __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(f + p * kFeat);
+#pragma unroll
+    for (int k = 0; k < kFeat / 2; k++) o[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+  }
+}
+
+// L1 loss in log(1 + radiance): prediction = log(1 + base) + out[0:3].
+__global__ void loss_kernel(const float* __restrict__ out, const float4* __restrict__ noisy, const float4* __restrict__ target,
+                            bf16* __restrict__ dout, float* __restrict__ loss, long pixels, float scale) {
+  __shared__ float part[256];
+  float s = 0.0f;
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += (long)gridDim.x * blockDim.x) {
+    const float4 nz = noisy[p], tg = target[p];
+    const float nv[3] = {nz.x, nz.y, nz.z}, tv[3] = {tg.x, tg.y, tg.z};
+    __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(dout + p * kOutC);
+    float g[kOutC] = {};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float diff = log1pf(fmaxf(nv[c], 0.0f)) + out[p * kOutC + c] - log1pf(fmaxf(tv[c], 0.0f));
+      s += fabsf(diff);
+      g[c] = diff > 0.0f ? scale : (diff < 0.0f ? -scale : 0.0f);
+    }
+#pragma unroll
+    for (int k = 0; k < kOutC / 2; k++) d[k] = __floats2bfloat162_rn(g[2 * k], g[2 * k + 1]);
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(loss, part[0]);
+}
+
+__global__ void output_kernel(const float* __restrict__ out, const float4* __restrict__ noisy, float4* __restrict__ den, long pixels) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += (long)gridDim.x * blockDim.x) {
+    const float4 nz = noisy[p];
+    const float* o = out + p * kOutC;
+    den[p] = make_float4(expm1f(log1pf(fmaxf(nz.x, 0.0f)) + o[0]), expm1f(log1pf(fmaxf(nz.y, 0.0f)) + o[1]),
+                         expm1f(log1pf(fmaxf(nz.z, 0.0f)) + o[2]), 1.0f);
+  }
+}
+
+__global__ void accumulate_kernel(float* __restrict__ sum, const float* __restrict__ x, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) sum[i] += x[i];
+}
+__global__ void scale_kernel(float* __restrict__ x, long n, float s) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] *= s;
+}
+
+// ------------------------------------------------------------- parameters --
+// One layer's parameters inside the flat FP32 arrays: weights [cout][9][cin]
+// at woff, biases at boff.
+struct LayerParams {
+  int cin, cout;
+  long woff, boff;
+};
+
+// Hash-based normal deviates (Box-Muller over two hashed uniforms).
+__device__ __forceinline__ float hash_uniform(uint32_t i, uint32_t seed) {
+  uint32_t h = hashU(i * 2654435761u ^ hashU(seed));
+  return ((float)(h >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+__global__ void init_kernel(float* __restrict__ w, long count, float stdev, uint32_t seed) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x) {
+    const float u1 = hash_uniform((uint32_t)(2 * i), seed), u2 = hash_uniform((uint32_t)(2 * i + 1), seed);
+    w[i] = stdev * sqrtf(-2.0f * logf(u1)) * cosf(6.2831853f * u2);
+  }
+}
+
+// Adam on the flat parameters; writes the BF16 forward weights and the
+// rotated, transposed BF16 weights of the backward data pass.
+struct AdamArgs {
+  float* p;
+  float* g;
+  float* m;
+  float* v;
+  long count;
+  float lr, b1, b2, eps, c1, c2;  // c1 = 1 - b1^t, c2 = 1 - b2^t
+};
+__global__ void adam_kernel(AdamArgs a) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.count; i += (long)gridDim.x * blockDim.x) {
+    const float g = a.g[i];
+    const float m = a.b1 * a.m[i] + (1.0f - a.b1) * g;
+    const float v = a.b2 * a.v[i] + (1.0f - a.b2) * g * g;
+    a.m[i] = m;
+    a.v[i] = v;
+    a.p[i] -= a.lr * (m / a.c1) / (sqrtf(v / a.c2) + a.eps);
+    a.g[i] = 0.0f;
+  }
+}
+// wf[co][tap][ci] = p[woff + ...]; wb[ci][8 - tap][co] = the same value
+__global__ void cast_kernel(const float* __restrict__ p, bf16* __restrict__ wf, bf16* __restrict__ wb, int cin, int cout) {
+  const long total = (long)cout * 9 * cin;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int ci = (int)(i % cin);
+    const long q = i / cin;
+    const int tap = (int)(q % 9);
+    const int co = (int)(q / 9);
+    const bf16 v = __float2bfloat16(p[i]);
+    wf[i] = v;
+    wb[((size_t)ci * 9 + (8 - tap)) * cout + co] = v;
+  }
+}
+
+int cuda_fail(const char* what, cudaError_t e) {
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return ARBOR_ERR_CUDA;
+}
+#define DN_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(#call, e_); \
+  } while (0)
+
+dim3 ew_grid(long n) {
+  long b = (n + 255) / 256;
+  return dim3((unsigned)(b < 4096 ? (b > 0 ? b : 1) : 4096));
+}
+
+}  // namespace
+}  // namespace arbor
+
+using namespace arbor;
+
+// The network: 15 convolutions.
+namespace {
+constexpr int kLayers = 15;
+// (cin, cout, leaky ReLU) of each convolution, in forward order
+constexpr int kSpec[kLayers][3] = {
+    {kFeat, 32, 1}, {32, 32, 1},      // encoder level 0
+    {32, 64, 1},    {64, 64, 1},      // level 1
+    {64, 96, 1},    {96, 96, 1},      // level 2
+    {96, 128, 1},   {128, 128, 1},    // level 3
+    {224, 96, 1},   {96, 96, 1},      // decoder level 2 (96 skip + 128 up)
+    {160, 64, 1},   {64, 64, 1},      // level 1 (64 + 96)
+    {96, 32, 1},    {32, 32, 1},      // level 0 (32 + 64)
+    {32, kOutC, 0},                   // output (3 of 16 channels used)
+};
+// activation tensors
+enum Act {
+  aF, aE0a, aE0, aP1, aE1a, aE1, aP2, aE2a, aE2, aP3, aB3a, aB3, aC2, aD2a, aD2, aC1, aD1a, aD1, aC0, aD0a, aD0, kActs
+};
+struct ActSpec {
+  int level, channels;
+};
+constexpr ActSpec kAct[kActs] = {{0, kFeat}, {0, 32}, {0, 32}, {1, 32}, {1, 64},  {1, 64}, {2, 64}, {2, 96}, {2, 96}, {3, 96}, {3, 128},
+                                 {3, 128},   {2, 224}, {2, 96}, {2, 96}, {1, 160}, {1, 64}, {1, 64}, {0, 96}, {0, 32}, {0, 32}};
+// input and output tensor of each convolution (the output layer writes `out`)
+constexpr int kIn[kLayers] = {aF, aE0a, aP1, aE1a, aP2, aE2a, aP3, aB3a, aC2, aD2a, aC1, aD1a, aC0, aD0a, aD0};
+constexpr int kOut[kLayers] = {aE0a, aE0, aE1a, aE1, aE2a, aE2, aB3a, aB3, aD2a, aD2, aD1a, aD1, aD0a, aD0, -1};
+}  // namespace
+
+struct arbor_denoiser {
+  cudaStream_t stream = nullptr;
+  int max_batch = 0, max_w = 0, max_h = 0;
+  long param_count = 0;
+  LayerParams layer[kLayers];
+  float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;  // FP32 parameters, gradients, moments
+  bf16 *wf = nullptr, *wb = nullptr;                              // BF16 forward / backward-data weights
+  long wf_off[kLayers];
+  bf16* act[kActs] = {};
+  bf16* grad[kActs] = {};
+  bf16* dcat[3] = {};     // skip gradients from the concat, levels 0..2
+  float* out = nullptr;   // network output, kOutC FP32 channels
+  bf16* dout = nullptr;
+  float* loss = nullptr;  // device scalar
+  float loss_host = 0.0f;
+  int* err = nullptr;     // device flag: a tcgen05 wait gave up
+  bool tc = true;         // forward convolutions on tcgen05
+  long steps = 0;
+  size_t allocated = 0;
+};
+
+namespace {
+
+long level_pixels(const arbor_denoiser* d, int level, int batch, int w, int h) { return (long)batch * (w >> level) * (h >> level); }
+
+int launch_conv(const ConvArgs& a, cudaStream_t s) {
+  const dim3 grid((unsigned)(((a.w + 7) / 8) * ((a.h + 7) / 8)), 1, (unsigned)a.n);
+  const int kc = a.cin % 32 == 0 ? 32 : 16;
+  const int nt = a.cout % 64 == 0 ? 8 : (a.cout % 32 == 0 ? 4 : 2);
+  dim3 g = grid;
+  g.y = (unsigned)(a.cout / (nt * 8));
+#define DN_CONV(KC, NT)                                                                                                 \
+  do {                                                                                                                  \
+    static bool ready = false;                                                                                          \
+    if (!ready) {                                                                                                       \
+      if (cudaFuncSetAttribute(conv_kernel<KC, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem_bytes<KC, NT>()) != \
+          cudaSuccess)                                                                                                  \
+        return cuda_fail("cudaFuncSetAttribute (conv)", cudaGetLastError());                                            \
+      ready = true;                                                                                                     \
+    }                                                                                                                   \
+    conv_kernel<KC, NT><<<g, 128, conv_smem_bytes<KC, NT>(), s>>>(a);                                                   \
+  } while (0)
+  if (kc == 32 && nt == 8) DN_CONV(32, 8);
+  else if (kc == 32 && nt == 4) DN_CONV(32, 4);
+  else if (kc == 32 && nt == 2) DN_CONV(32, 2);
+  else if (kc == 16 && nt == 8) DN_CONV(16, 8);
+  else if (kc == 16 && nt == 4) DN_CONV(16, 4);
+  else DN_CONV(16, 2);
+#undef DN_CONV
+  count_launch();
+  return check_launch("conv_kernel");
+}
+
+// The forward convolutions on tcgen05 (N = cout up to 128); false when the
+// layer shape has no tcgen05 form here (the caller then uses conv_kernel).
+template <int N, int CC>
+int launch_tc(const ConvArgs& a, int* err, cudaStream_t s) {
+  static bool ready = false;
+  if (!ready) {
+    if (cudaFuncSetAttribute(conv_tc_kernel<N, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_tc_smem_bytes<N, CC>()) != cudaSuccess)
+      return cuda_fail("cudaFuncSetAttribute (conv_tc)", cudaGetLastError());
+    ready = true;
+  }
+  const dim3 grid((unsigned)(((a.w + 127) / 128) * a.h * a.n));
+  conv_tc_kernel<N, CC><<<grid, 128, conv_tc_smem_bytes<N, CC>(), s>>>(a, err);
+  count_launch();
+  return check_launch("conv_tc_kernel");
+}
+bool tc_shape(const ConvArgs& a) { return a.cout == 16 || a.cout == 32 || a.cout == 64 || a.cout == 96 || a.cout == 128; }
+int launch_conv_tc(const ConvArgs& a, int* err, cudaStream_t s) {
+  const bool c32 = a.cin % 32 == 0;
+  switch (a.cout) {
+    case 16: return c32 ? launch_tc<16, 32>(a, err, s) : launch_tc<16, 16>(a, err, s);
+    case 32: return c32 ? launch_tc<32, 32>(a, err, s) : launch_tc<32, 16>(a, err, s);
+    case 64: return c32 ? launch_tc<64, 32>(a, err, s) : launch_tc<64, 16>(a, err, s);
+    case 96: return c32 ? launch_tc<96, 32>(a, err, s) : launch_tc<96, 16>(a, err, s);
+    default: return c32 ? launch_tc<128, 32>(a, err, s) : launch_tc<128, 16>(a, err, s);
+  }
+}
+
+int launch_wgrad(const bf16* dy, const bf16* x, float* dw, int cin, int cout, int n, int h, int w, cudaStream_t s) {
+  WgradArgs a{dy, x, dw, cin, cout, n, h, w, 0};
+  const long pixels = (long)n * h * w;
+  const int ci_tile = cin % 32 == 0 ? 32 : 16;
+  const int base = ((cout + 63) / 64) * 9 * (cin / ci_tile);
+  long split = 1184 / base;
+  if (split < 1) split = 1;
+  long per = (pixels + split - 1) / split;
+  per = (per + 31) / 32 * 32;
+  if (per < 256) per = 256;
+  a.pixels_per_cta = (int)per;
+  const dim3 grid((unsigned)((pixels + per - 1) / per), (unsigned)((cout + 63) / 64), (unsigned)(9 * (cin / ci_tile)));
+  if (ci_tile == 32)
+    wgrad_kernel<32><<<grid, 128, 0, s>>>(a);
+  else
+    wgrad_kernel<16><<<grid, 128, 0, s>>>(a);
+  count_launch();
+  return check_launch("wgrad_kernel");
+}
+
+int check_size(const char* what, int batch, int w, int h, const arbor_denoiser* d) {
+  if (batch < 1 || w < 8 || h < 8 || w % 8 || h % 8) {
+    set_error("%s: batch >= 1 and width, height multiples of 8 are required (got %d x %d x %d)", what, batch, w, h);
+    return ARBOR_ERR_VALUE;
+  }
+  if ((long)batch * w * h > (long)d->max_batch * d->max_w * d->max_h) {
+    set_error("%s: %d x %d x %d pixels exceed the %d x %d x %d the denoiser was created for", what, batch, w, h, d->max_batch, d->max_w,
+              d->max_h);
+    return ARBOR_ERR_LIMIT;
+  }
+  return ARBOR_OK;
+}
+
+int cast_weights(arbor_denoiser* d) {
+  for (int l = 0; l < kLayers; l++) {
+    const LayerParams& L = d->layer[l];
+    cast_kernel<<<ew_grid((long)L.cout * 9 * L.cin), 256, 0, d->stream>>>(d->p + L.woff, d->wf + d->wf_off[l], d->wb + d->wf_off[l], L.cin,
+                                                                          L.cout);
+    count_launch();
+  }
+  return check_launch("cast_kernel");
+}
+
+// Forward pass over `features` (batch x h x w x 16 BF16); the output lands in d->out.
+int forward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
+  cudaStream_t s = d->stream;
+  const bf16* in[kActs];
+  for (int k = 0; k < kActs; k++) in[k] = d->act[k];
+  in[aF] = features;
+  auto conv = [&](int l) {
+    const LayerParams& L = d->layer[l];
+    const int lv = kAct[kIn[l]].level;
+    ConvArgs a{in[kIn[l]], d->wf + d->wf_off[l], d->p + L.boff,
+               kOut[l] < 0 ? (void*)d->out : (void*)d->act[kOut[l]], nullptr, L.cin, L.cout, batch, h >> lv, w >> lv, kSpec[l][2],
+               kOut[l] < 0 ? 1 : 0};
+    return d->tc && tc_shape(a) ? launch_conv_tc(a, d->err, s) : launch_conv(a, s);
+  };
+  auto pool = [&](int src, int dst) {
+    const int lv = kAct[src].level;
+    const long n = level_pixels(d, lv + 1, batch, w, h) * kAct[src].channels;
+    pool_kernel<<<ew_grid(n), 256, 0, s>>>(d->act[src], d->act[dst], batch, h >> lv, w >> lv, kAct[src].channels);
+    count_launch();
+    return check_launch("pool_kernel");
+  };
+  auto upcat = [&](int skip, int low, int dst) {
+    const int lv = kAct[skip].level;
+    const long n = level_pixels(d, lv, batch, w, h) * kAct[dst].channels;
+    upcat_kernel<<<ew_grid(n), 256, 0, s>>>(d->act[skip], d->act[low], d->act[dst], batch, h >> lv, w >> lv, kAct[skip].channels,
+                                            kAct[low].channels);
+    count_launch();
+    return check_launch("upcat_kernel");
+  };
+  int st;
+  if ((st = conv(0)) || (st = conv(1)) || (st = pool(aE0, aP1)) || (st = conv(2)) || (st = conv(3)) || (st = pool(aE1, aP2)) ||
+      (st = conv(4)) || (st = conv(5)) || (st = pool(aE2, aP3)) || (st = conv(6)) || (st = conv(7)) || (st = upcat(aE2, aB3, aC2)) ||
+      (st = conv(8)) || (st = conv(9)) || (st = upcat(aE1, aD2, aC1)) || (st = conv(10)) || (st = conv(11)) ||
+      (st = upcat(aE0, aD1, aC0)) || (st = conv(12)) || (st = conv(13)) || (st = conv(14)))
+    return st;
+  return ARBOR_OK;
+}
+
+// Backward pass from d->dout; accumulates into d->g.
+int backward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
+  cudaStream_t s = d->stream;
+  auto x_of = [&](int l) -> const bf16* { return kIn[l] == aF ? features : d->act[kIn[l]]; };
+  // weight and bias gradients of layer l from dY (its pre-activation gradient)
+  auto wgrad = [&](int l, const bf16* dy) {
+    const LayerParams& L = d->layer[l];
+    const int lv = kAct[kIn[l]].level;
+    if (int st = launch_wgrad(dy, x_of(l), d->g + L.woff, L.cin, L.cout, batch, h >> lv, w >> lv, s)) return st;
+    const long px = level_pixels(d, lv, batch, w, h);
+    bgrad_kernel<<<(unsigned)std::min<long>(1184, (px * L.cout + 255) / 256 + 1), 256, 0, s>>>(dy, d->g + L.boff, L.cout, px);
+    count_launch();
+    return check_launch("bgrad_kernel");
+  };
+  // input gradient of layer l: conv of dY with the rotated, transposed
+  // weights; mask_act: the input's activation derivative (or -1: none)
+  auto dgrad = [&](int l, const bf16* dy, bf16* dx, int mask_act) {
+    const LayerParams& L = d->layer[l];
+    const int lv = kAct[kIn[l]].level;
+    ConvArgs a{dy, d->wb + d->wf_off[l], nullptr, dx, mask_act >= 0 ? d->act[mask_act] : nullptr, L.cout, L.cin, batch, h >> lv, w >> lv, 0, 0};
+    return launch_conv(a, s);
+  };
+  auto upcat_back = [&](int cat, int skip_level, int low) {
+    const int lv = kAct[cat].level;
+    const int cs = kAct[cat].channels - kAct[low].channels, cl = kAct[low].channels;
+    const long n = level_pixels(d, lv, batch, w, h) * cs + level_pixels(d, lv + 1, batch, w, h) * cl;
+    upcat_back_kernel<<<ew_grid(n), 256, 0, s>>>(d->grad[cat], d->act[low], d->dcat[skip_level], d->grad[low], batch, h >> lv, w >> lv, cs,
+                                                 cl);
+    count_launch();
+    return check_launch("upcat_back_kernel");
+  };
+  auto pool_back = [&](int pooled, int skip, int skip_level) {
+    const int lv = kAct[skip].level;
+    const long n = level_pixels(d, lv, batch, w, h) * kAct[skip].channels;
+    pool_back_kernel<<<ew_grid(n), 256, 0, s>>>(d->grad[pooled], d->dcat[skip_level], d->act[skip], d->grad[skip], batch, h >> lv, w >> lv,
+                                                kAct[skip].channels);
+    count_launch();
+    return check_launch("pool_back_kernel");
+  };
+  int st;
+  // decoder level 0
+  if ((st = wgrad(14, d->dout)) || (st = dgrad(14, d->dout, d->grad[aD0], aD0))) return st;
+  if ((st = wgrad(13, d->grad[aD0])) || (st = dgrad(13, d->grad[aD0], d->grad[aD0a], aD0a))) return st;
+  if ((st = wgrad(12, d->grad[aD0a])) || (st = dgrad(12, d->grad[aD0a], d->grad[aC0], -1))) return st;
+  if ((st = upcat_back(aC0, 0, aD1))) return st;
+  // decoder level 1
+  if ((st = wgrad(11, d->grad[aD1])) || (st = dgrad(11, d->grad[aD1], d->grad[aD1a], aD1a))) return st;
+  if ((st = wgrad(10, d->grad[aD1a])) || (st = dgrad(10, d->grad[aD1a], d->grad[aC1], -1))) return st;
+  if ((st = upcat_back(aC1, 1, aD2))) return st;
+  // decoder level 2
+  if ((st = wgrad(9, d->grad[aD2])) || (st = dgrad(9, d->grad[aD2], d->grad[aD2a], aD2a))) return st;
+  if ((st = wgrad(8, d->grad[aD2a])) || (st = dgrad(8, d->grad[aD2a], d->grad[aC2], -1))) return st;
+  if ((st = upcat_back(aC2, 2, aB3))) return st;
+  // bottleneck
+  if ((st = wgrad(7, d->grad[aB3])) || (st = dgrad(7, d->grad[aB3], d->grad[aB3a], aB3a))) return st;
+  if ((st = wgrad(6, d->grad[aB3a])) || (st = dgrad(6, d->grad[aB3a], d->grad[aP3], -1))) return st;
+  if ((st = pool_back(aP3, aE2, 2))) return st;
+  // encoder level 2
+  if ((st = wgrad(5, d->grad[aE2])) || (st = dgrad(5, d->grad[aE2], d->grad[aE2a], aE2a))) return st;
+  if ((st = wgrad(4, d->grad[aE2a])) || (st = dgrad(4, d->grad[aE2a], d->grad[aP2], -1))) return st;
+  if ((st = pool_back(aP2, aE1, 1))) return st;
+  // encoder level 1
+  if ((st = wgrad(3, d->grad[aE1])) || (st = dgrad(3, d->grad[aE1], d->grad[aE1a], aE1a))) return st;
+  if ((st = wgrad(2, d->grad[aE1a])) || (st = dgrad(2, d->grad[aE1a], d->grad[aP1], -1))) return st;
+  if ((st = pool_back(aP1, aE0, 0))) return st;
+  // encoder level 0
+  if ((st = wgrad(1, d->grad[aE0])) || (st = dgrad(1, d->grad[aE0], d->grad[aE0a], aE0a))) return st;
+  if ((st = wgrad(0, d->grad[aE0a]))) return st;
+  return ARBOR_OK;
+}
+
+int live(arbor_denoiser* d, const char* what) {
+  if (d == nullptr) {
+    set_error("%s: denoiser is NULL", what);
+    return ARBOR_ERR_NULL;
+  }
+  return ARBOR_OK;
+}
+
+}  // namespace
+
+extern "C" int arbor_denoiser_create(arbor_denoiser** out, int max_batch, int max_width, int max_height, uint32_t seed, arbor_stream stream) {
+  if (out == nullptr) {
+    set_error("arbor_denoiser_create: out is NULL");
+    return ARBOR_ERR_NULL;
+  }
+  *out = nullptr;
+  if (max_batch < 1 || max_width < 8 || max_height < 8 || max_width % 8 || max_height % 8) {
+    set_error("arbor_denoiser_create: batch >= 1 and width, height multiples of 8 are required (got %d x %d x %d)", max_batch, max_width,
+              max_height);
+    return ARBOR_ERR_VALUE;
+  }
+  if ((long)max_batch * max_width * max_height > (1L << 26)) {
+    set_error("arbor_denoiser_create: %d x %d x %d pixels exceed 2^26", max_batch, max_width, max_height);
+    return ARBOR_ERR_LIMIT;
+  }
+  if (!arbor_device_ready()) {
+    set_error("arbor_denoiser_create: no sm_100 CUDA device is available");
+    return ARBOR_ERR_NO_DEVICE;
+  }
+  arbor_denoiser* d = new (std::nothrow) arbor_denoiser();
+  if (d == nullptr) {
+    set_error("arbor_denoiser_create: out of host memory");
+    return ARBOR_ERR_LIMIT;
+  }
+  auto fail = [&](int s) {
+    arbor_denoiser_destroy(d);
+    return s;
+  };
+  d->stream = stream;
+  d->max_batch = max_batch;
+  d->max_w = max_width;
+  d->max_h = max_height;
+  long off = 0, woff = 0;
+  for (int l = 0; l < kLayers; l++) {
+    LayerParams& L = d->layer[l];
+    L.cin = kSpec[l][0];
+    L.cout = kSpec[l][1];
+    L.woff = off;
+    off += (long)L.cout * 9 * L.cin;
+    L.boff = off;
+    off += L.cout;
+    d->wf_off[l] = woff;
+    woff += (long)L.cout * 9 * L.cin;
+  }
+  d->param_count = off;
+  cudaError_t ce;
+  auto alloc = [&](void** ptr, size_t bytes) {
+    ce = cudaMalloc(ptr, bytes);
+    if (ce == cudaSuccess) d->allocated += bytes;
+    return ce == cudaSuccess;
+  };
+  const size_t pb = (size_t)off * 4;
+  if (!alloc((void**)&d->p, pb) || !alloc((void**)&d->g, pb) || !alloc((void**)&d->m, pb) || !alloc((void**)&d->v, pb) ||
+      !alloc((void**)&d->wf, (size_t)woff * 2) || !alloc((void**)&d->wb, (size_t)woff * 2) || !alloc((void**)&d->loss, 4) ||
+      !alloc((void**)&d->err, 4))
+    return fail(cuda_fail("cudaMalloc (denoiser parameters)", ce));
+  const long px0 = (long)max_batch * max_width * max_height;
+  for (int k = 0; k < kActs; k++) {
+    const size_t bytes = (size_t)(px0 >> (2 * kAct[k].level)) * kAct[k].channels * 2;
+    if (k != aF && !alloc((void**)&d->act[k], bytes)) return fail(cuda_fail("cudaMalloc (denoiser activations)", ce));
+    if (!alloc((void**)&d->grad[k], bytes)) return fail(cuda_fail("cudaMalloc (denoiser gradients)", ce));
+  }
+  const int skips[3] = {aE0, aE1, aE2};
+  for (int lv = 0; lv < 3; lv++)
+    if (!alloc((void**)&d->dcat[lv], (size_t)(px0 >> (2 * lv)) * kAct[skips[lv]].channels * 2))
+      return fail(cuda_fail("cudaMalloc (denoiser concat gradients)", ce));
+  if (!alloc((void**)&d->out, (size_t)px0 * kOutC * 4) || !alloc((void**)&d->dout, (size_t)px0 * kOutC * 2))
+    return fail(cuda_fail("cudaMalloc (denoiser output)", ce));
+  // He-normal weights (the output layer 10x smaller), zero biases and moments
+  if ((ce = cudaMemsetAsync(d->err, 0, 4, stream)) != cudaSuccess || (ce = cudaMemsetAsync(d->p, 0, pb, stream)) != cudaSuccess ||
+      (ce = cudaMemsetAsync(d->g, 0, pb, stream)) != cudaSuccess ||
+      (ce = cudaMemsetAsync(d->m, 0, pb, stream)) != cudaSuccess || (ce = cudaMemsetAsync(d->v, 0, pb, stream)) != cudaSuccess)
+    return fail(cuda_fail("cudaMemsetAsync", ce));
+  for (int l = 0; l < kLayers; l++) {
+    const LayerParams& L = d->layer[l];
+    const float stdev = sqrtf(2.0f / (9.0f * L.cin)) * (l == kLayers - 1 ? 0.1f : 1.0f);
+    init_kernel<<<ew_grid((long)L.cout * 9 * L.cin), 256, 0, stream>>>(d->p + L.woff, (long)L.cout * 9 * L.cin, stdev, seed * 977u + l);
+    count_launch();
+  }
+  if (int st = cast_weights(d)) return fail(st);
+  if ((ce = cudaStreamSynchronize(stream)) != cudaSuccess) return fail(cuda_fail("cudaStreamSynchronize", ce));
+  *out = d;
+  return ARBOR_OK;
+}
+
+namespace {
+// A tcgen05 wait that gave up leaves its flag set: report it (and clear it).
+int check_err(arbor_denoiser* d, const char* what) {
+  int e = 0;
+  DN_CUDA(cudaMemcpyAsync(&e, d->err, 4, cudaMemcpyDeviceToHost, d->stream));
+  DN_CUDA(cudaStreamSynchronize(d->stream));
+  if (e) {
+    cudaMemsetAsync(d->err, 0, 4, d->stream);
+    set_error("%s: a tensor-core convolution timed out waiting for its MMAs", what);
+    return ARBOR_ERR_TIMEOUT;
+  }
+  return ARBOR_OK;
+}
+}  // namespace
+
+extern "C" int arbor_denoiser_set_backend(arbor_denoiser* d, int tcgen05) {
+  if (int s = live(d, "arbor_denoiser_set_backend")) return s;
+  d->tc = tcgen05 != 0;
+  return ARBOR_OK;
+}
+
+extern "C" int arbor_denoiser_param_count(arbor_denoiser* d, size_t* count) {
+  if (int s = live(d, "arbor_denoiser_param_count")) return s;
+  if (count == nullptr) {
+    set_error("arbor_denoiser_param_count: count is NULL");
+    return ARBOR_ERR_NULL;
+  }
+  *count = (size_t)d->param_count;
+  return ARBOR_OK;
+}
+
+extern "C" int arbor_denoiser_get_params(arbor_denoiser* d, float* host, size_t count) {
+  if (int s = live(d, "arbor_denoiser_get_params")) return s;
+  if (host == nullptr || count < (size_t)d->param_count) {
+    set_error("arbor_denoiser_get_params: need room for %ld floats", d->param_count);
+    return host == nullptr ? ARBOR_ERR_NULL : ARBOR_ERR_LIMIT;
+  }
+  DN_CUDA(cudaMemcpyAsync(host, d->p, (size_t)d->param_count * 4, cudaMemcpyDeviceToHost, d->stream));
+  DN_CUDA(cudaStreamSynchronize(d->stream));
+  return ARBOR_OK;
+}
+
+extern "C" int arbor_denoiser_set_params(arbor_denoiser* d, const float* host, size_t count) {
+  if (int s = live(d, "arbor_denoiser_set_params")) return s;
+  if (host == nullptr || count != (size_t)d->param_count) {
+    set_error("arbor_denoiser_set_params: expected %ld floats", d->param_count);
+    return host == nullptr ? ARBOR_ERR_NULL : ARBOR_ERR_VALUE;
+  }
+  for (size_t i = 0; i < count; i++)
+    if (!std::isfinite(host[i])) {
+      set_error("arbor_denoiser_set_params: parameter %zu is not finite", i);
+      return ARBOR_ERR_VALUE;
+    }
+  DN_CUDA(cudaMemcpyAsync(d->p, host, count * 4, cudaMemcpyHostToDevice, d->stream));
+  if (int st = cast_weights(d)) return st;
+  DN_CUDA(cudaStreamSynchronize(d->stream));
+  return ARBOR_OK;
+}
+
+extern "C" int arbor_denoiser_features(const float* Linear, const float* Guide, const float* Normal, const float* Hit, const float* Filtered,
+                                       int width, int height, uint16_t* features, arbor_stream stream) {
+  bool empty;
+  if (int s = check_image("arbor_denoiser_features", width, height, &empty)) return s;
+  const size_t img = empty ? 0 : image_bytes(width, height);
+  const Binding b[] = {{Linear, img, false, 16, "Linear"},
+                       {Guide, img, false, 16, "Guide"},
+                       {Normal, img, false, 16, "Normal"},
+                       {Hit, img, false, 16, "Hit"},
+                       {Filtered, img, false, 16, "Filtered"},
+                       {features, (size_t)width * height * kFeat * 2, true, 16, "features"}};
+  if (int s = check_bindings("arbor_denoiser_features", b)) return s;
+  if (empty) return ARBOR_OK;
+  const long px = (long)width * height;
+  features_kernel<<<ew_grid(px), 256, 0, stream>>>(reinterpret_cast<const float4*>(Linear), reinterpret_cast<const float4*>(Guide),
+                                                   reinterpret_cast<const float4*>(Normal), reinterpret_cast<const float4*>(Hit),
+                                                   reinterpret_cast<const float4*>(Filtered), reinterpret_cast<bf16*>(features), px);
+  count_launch();
+  return check_launch("arbor_denoiser_features");
+}
+
+extern "C" int arbor_denoiser_train_step(arbor_denoiser* d, const uint16_t* features, const float* base, const float* target, int batch,
+                                         int width, int height, float lr, float* loss) {
+  if (int s = live(d, "arbor_denoiser_train_step")) return s;
+  if (features == nullptr || base == nullptr || target == nullptr) {
+    set_error("arbor_denoiser_train_step: features, base and target must not be NULL");
+    return ARBOR_ERR_NULL;
+  }
+  if (int s = check_size("arbor_denoiser_train_step", batch, width, height, d)) return s;
+  if (!(lr > 0.0f) || !std::isfinite(lr)) {
+    set_error("arbor_denoiser_train_step: lr must be positive and finite");
+    return ARBOR_ERR_VALUE;
+  }
+  cudaStream_t s = d->stream;
+  const bf16* f = reinterpret_cast<const bf16*>(features);
+  if (int st = forward(d, f, batch, width, height)) return st;
+  const long px = (long)batch * width * height;
+  DN_CUDA(cudaMemsetAsync(d->loss, 0, 4, s));
+  loss_kernel<<<ew_grid(px), 256, 0, s>>>(d->out, reinterpret_cast<const float4*>(base), reinterpret_cast<const float4*>(target), d->dout,
+                                          d->loss, px, 1.0f / (float)(px * 3));
+  count_launch();
+  if (int st = check_launch("loss_kernel")) return st;
+  if (int st = backward(d, f, batch, width, height)) return st;
+  d->steps++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  AdamArgs a{d->p, d->g, d->m, d->v, d->param_count, lr, b1, b2, 1e-8f, 1.0f - powf(b1, (float)d->steps), 1.0f - powf(b2, (float)d->steps)};
+  adam_kernel<<<ew_grid(d->param_count), 256, 0, s>>>(a);
+  count_launch();
+  if (int st = check_launch("adam_kernel")) return st;
+  if (int st = cast_weights(d)) return st;
+  if (loss) {
+    DN_CUDA(cudaMemcpyAsync(&d->loss_host, d->loss, 4, cudaMemcpyDeviceToHost, s));
+    DN_CUDA(cudaStreamSynchronize(s));
+    *loss = d->loss_host / (float)(px * 3);
+    return check_err(d, "arbor_denoiser_train_step");
+  }
+  return ARBOR_OK;
+}
+
+extern "C" int arbor_denoiser_infer(arbor_denoiser* d, const uint16_t* features, const float* base, float* denoised, int width, int height) {
+  if (int s = live(d, "arbor_denoiser_infer")) return s;
+  if (features == nullptr || base == nullptr || denoised == nullptr) {
+    set_error("arbor_denoiser_infer: features, base and denoised must not be NULL");
+    return ARBOR_ERR_NULL;
+  }
+  if (int s = check_size("arbor_denoiser_infer", 1, width, height, d)) return s;
+  if (int st = forward(d, reinterpret_cast<const bf16*>(features), 1, width, height)) return st;
+  const long px = (long)width * height;
+  output_kernel<<<ew_grid(px), 256, 0, d->stream>>>(d->out, reinterpret_cast<const float4*>(base), reinterpret_cast<float4*>(denoised), px);
+  count_launch();
+  return check_launch("output_kernel");
+}
+
+extern "C" int arbor_denoiser_check(arbor_denoiser* d) {
+  if (int s = live(d, "arbor_denoiser_check")) return s;
+  return check_err(d, "arbor_denoiser_check");
+}
+
+extern "C" int arbor_denoiser_destroy(arbor_denoiser* d) {
+  if (d == nullptr) return ARBOR_OK;
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  void* bufs[] = {d->p, d->g, d->m, d->v, d->wf, d->wb, d->out, d->dout, d->loss, d->err, d->dcat[0], d->dcat[1], d->dcat[2]};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  for (int k = 0; k < kActs; k++) {
+    if (d->act[k]) cudaFree(d->act[k]);
+    if (d->grad[k]) cudaFree(d->grad[k]);
+  }
+  delete d;
+  return ARBOR_OK;
+}
+
+extern "C" int arbor_accumulate(float* sum, const float* x, size_t count, float scale, arbor_stream stream) {
+  if (sum == nullptr || x == nullptr) {
+    set_error("arbor_accumulate: sum and x must not be NULL");
+    return count == 0 ? ARBOR_OK : ARBOR_ERR_NULL;
+  }
+  if (!std::isfinite(scale)) {
+    set_error("arbor_accumulate: scale must be finite");
+    return ARBOR_ERR_VALUE;
+  }
+  if (count == 0) return ARBOR_OK;
+  if (scale != 1.0f) {
+    scale_kernel<<<ew_grid((long)count), 256, 0, stream>>>(sum, (long)count, scale);
+    count_launch();
+  }
+  accumulate_kernel<<<ew_grid((long)count), 256, 0, stream>>>(sum, x, (long)count);
+  count_launch();
+  return check_launch("arbor_accumulate");
+}

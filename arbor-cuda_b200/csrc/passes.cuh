@@ -201,6 +201,7 @@ __device__ float spec_ggx(f3 n, f3 v, f3 l, float rough) {
 // before haze is (direct * visibility) * (4.8, 4.2, 3.1) + albedo * ambient.
 struct Shading {
   f3 direct, ambientTerm, skyc, guide, origin, light, debug;
+  f3 normal;    // shading normal (zero for sky), the G-buffer normal
   float haze;
   bool final;   // colour is `debug` (sky pixel or debug view mode): no visibility needed
   bool shadow;  // visibility must be traced
@@ -225,6 +226,7 @@ __device__ __noinline__ void shade_pre(const float* P, const Camera& cam, const 
   o.skyc = sky(rd, sun);
   o.guide = mk(1.0f, 1.0f, 1.0f);
   o.shadow = false;
+  o.normal = mk(0.0f, 0.0f, 0.0f);
   if (!(t < kFar)) {
     o.final = true;
     o.debug = o.skyc;
@@ -257,6 +259,7 @@ __device__ __noinline__ void shade_pre(const float* P, const Camera& cam, const 
     float nz = (noise_h(p.x * 18.0f, (p.z + e) * 18.0f, h133) - noise_h(p.x * 18.0f, (p.z - e) * 18.0f, h133)) * 0.18f;
     n = norm3(mk(nx, 1.0f, nz));
   }
+  o.normal = n;
   f3 albedo = surface_color(P, id, id >= 0 ? localP : p, localFp, time + phase, wind);
   if (kForestScene && tree >= 0) {
     int ts = inst[tree].seed;
@@ -334,6 +337,7 @@ struct ShadePolicy {
   const Camera* cam;
   const Instance* inst;
   const float* Hit;
+  float* Normal;  // nullable: G-buffer normal output
   int width, height;
   int pixel, seg;
   f3 trans;
@@ -356,6 +360,7 @@ struct ShadePolicy {
     f3 col = shade_post(sh, visibility);
     reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
     reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);
+    if (Normal) reinterpret_cast<float4*>(Normal)[pixel] = make_float4(sh.normal.x, sh.normal.y, sh.normal.z, 0.0f);
   }
   __device__ __forceinline__ void done(Ray& r) {
     int id = (int)r.found;
@@ -380,10 +385,11 @@ struct ShadePolicy {
 template <bool kForestScene, class WB>
 __device__ __forceinline__ void shade_tile(const TraceCtx& c, const Camera& cam, const Instance* inst, WB& b, const float* __restrict__ P,
                                            const float* __restrict__ Hit, float* __restrict__ Linear, float* __restrict__ Guide, int width,
-                                           int height, int x0, int y0, int tw) {
+                                           int height, int x0, int y0, int tw, float* __restrict__ Normal = nullptr) {
   int x, y;
   tile_pixel_at(threadIdx.x, x0, y0, tw, x, y);
   ShadePolicy<kForestScene> policy;
+  policy.Normal = Normal;
   policy.P = P;
   policy.Linear = Linear;
   policy.Guide = Guide;

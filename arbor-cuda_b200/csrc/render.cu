@@ -23,14 +23,14 @@ template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock, 2) shade_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                           const uint32_t* __restrict__ Order, const float* __restrict__ C,
                                                           const float* __restrict__ Hit, float* __restrict__ Linear,
-                                                          float* __restrict__ Guide, int width, int height) {
+                                                          float* __restrict__ Guide, float* __restrict__ Normal, int width, int height) {
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
   __shared__ Camera cam;
   __shared__ Instance inst[kForestScene ? kForest : 1];
   block_setup(C, cam, inst, kForestScene);
   const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
-  shade_tile<kForestScene>(c, cam, inst, b, P, Hit, Linear, Guide, width, height, blockIdx.x * kTile, blockIdx.y * kTile, kTile);
+  shade_tile<kForestScene>(c, cam, inst, b, P, Hit, Linear, Guide, width, height, blockIdx.x * kTile, blockIdx.y * kTile, kTile, Normal);
 }
 
 // Persistent form of the trace: a grid of (SMs x 2) CTAs, each taking every
@@ -130,7 +130,7 @@ int trace_entry(const char* name, bool forest, const float* P, const float* Node
 }
 
 int shade_entry(const char* name, bool forest, const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit,
-                float* Linear, float* Guide, int width, int height, cudaStream_t stream) {
+                float* Linear, float* Guide, int width, int height, cudaStream_t stream, float* Normal = nullptr) {
   bool empty;
   if (int s = check_image(name, width, height, &empty)) return s;
   size_t img = empty ? 0 : image_bytes(width, height);
@@ -138,6 +138,11 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
                        {C, kC, false, 4, "C"},          {Hit, img, false, 16, "Hit"},        {Linear, img, true, 16, "Linear"},
                        {Guide, img, true, 16, "Guide"}};
   if (int s = check_bindings(name, b)) return s;
+  if (Normal != nullptr) {
+    const Binding g[] = {{P, kP, false, 16, "P"}, {Hit, img, false, 16, "Hit"}, {Linear, img, true, 16, "Linear"},
+                         {Guide, img, true, 16, "Guide"}, {Normal, img, true, 16, "Normal"}};
+    if (int s = check_bindings(name, g)) return s;
+  }
   if (empty) return ARBOR_OK;
   if (!batch_smem_ready(forest ? (const void*)shade_kernel<true> : (const void*)shade_kernel<false>)) {
     set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
@@ -147,9 +152,9 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
   // normals) is long, and refilling lanes one by one ran it with few lanes
   // active (measured slower than tiles).
   if (forest)
-    shade_kernel<true><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+    shade_kernel<true><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, Normal, width, height);
   else
-    shade_kernel<false><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+    shade_kernel<false><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, Normal, width, height);
   count_launch();
   return check_launch(name);
 }
@@ -170,6 +175,14 @@ extern "C" int arbor_traceTreePixels(const float* P, const float* Nodes, const u
 extern "C" int arbor_shadePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear,
                                  float* Guide, int width, int height, arbor_stream stream) {
   return shade_entry("arbor_shadePixels", true, P, Nodes, Order, C, Hit, Linear, Guide, width, height, stream);
+}
+extern "C" int arbor_shadeGBuffer(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear,
+                                  float* Guide, float* Normal, int width, int height, arbor_stream stream) {
+  if (Normal == nullptr && width > 0 && height > 0) {
+    set_error("arbor_shadeGBuffer: buffer Normal is NULL");
+    return ARBOR_ERR_NULL;
+  }
+  return shade_entry("arbor_shadeGBuffer", true, P, Nodes, Order, C, Hit, Linear, Guide, width, height, stream, Normal);
 }
 extern "C" int arbor_shadeTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear,
                                      float* Guide, int width, int height, arbor_stream stream) {

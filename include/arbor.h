@@ -191,6 +191,12 @@ ARBOR_API int arbor_buildScene(int seed, float* B, float* P, uint32_t* Keys, uin
 ARBOR_API int arbor_traceTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height, arbor_stream stream);
 ARBOR_API int arbor_shadeTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, arbor_stream stream);
 
+/* shadePixels (Arbor.cu:277-289) that also writes the shading normal of
+ * each pixel (world space, facing the camera; zero for sky) into Normal
+ * (W*H float4, .w = 0): the G-buffer the learned denoiser reads.  No
+ * reference counterpart: the reference keeps the normal inside shadePixels. */
+ARBOR_API int arbor_shadeGBuffer(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, float* Normal, int width, int height, arbor_stream stream);
+
 /* filterLighting followed by resolvePixels in one launch; writes Filtered,
  * History and Pixels exactly as the two separate entries do. */
 ARBOR_API int arbor_filterResolve(const float* Linear, const float* Guide, const float* Hit, float* Filtered, float* History, uint32_t* Pixels, const float* C, int width, int height, arbor_stream stream);
@@ -324,6 +330,49 @@ ARBOR_API int arbor_batch_inspect(arbor_batch* b, arbor_batch_info* info);
 /* Copies every view's Pixels, view after view, into host memory and waits. */
 ARBOR_API int arbor_batch_read_pixels(arbor_batch* b, uint32_t* host, size_t count);
 ARBOR_API int arbor_batch_destroy(arbor_batch* b);
+
+
+/* ---------------------------------------------------------------------------
+ * Learned denoiser (no reference counterpart; the reference's denoiser is
+ * filterLighting, Arbor.cu:292-302, which stays available): a 4-level
+ * convolutional encoder-decoder (channels 32/64/96/128, 3x3 kernels, leaky
+ * ReLU) over 16 BF16 feature channels per pixel (log(1 + radiance), albedo,
+ * normal, log(1 + depth), log(1 + filterLighting's radiance)), predicting
+ * log(1 + radiance) as a correction of a base image (filterLighting's
+ * output at the same sample count).  BF16 weights and activations, tensor-core products
+ * accumulated in FP32, FP32 master weights and Adam moments; trained and
+ * run by this library's own forward and backward kernels.  Image sizes are
+ * multiples of 8.  All calls run on the stream given at creation.
+ * ------------------------------------------------------------------------- */
+typedef struct arbor_denoiser arbor_denoiser;
+
+/* Creates the network (He-normal weights from `seed`) with working buffers
+ * for up to max_batch images of max_width x max_height pixels. */
+ARBOR_API int arbor_denoiser_create(arbor_denoiser** out, int max_batch, int max_width, int max_height, uint32_t seed, arbor_stream stream);
+ARBOR_API int arbor_denoiser_param_count(arbor_denoiser* d, size_t* count);
+/* FP32 parameters, layer after layer: weights [cout][3][3][cin], then biases. */
+ARBOR_API int arbor_denoiser_get_params(arbor_denoiser* d, float* host, size_t count);
+ARBOR_API int arbor_denoiser_set_params(arbor_denoiser* d, const float* host, size_t count);
+/* Packs one image's features (W*H*16 BF16, as uint16_t) from the 1-spp
+ * Linear, Guide (albedo), Normal (arbor_shadeGBuffer), Hit (depth) and
+ * Filtered (filterLighting of that sample). */
+ARBOR_API int arbor_denoiser_features(const float* Linear, const float* Guide, const float* Normal, const float* Hit, const float* Filtered, int width, int height, uint16_t* features, arbor_stream stream);
+/* One Adam step on a batch: features (batch images back to back), the base
+ * image the network corrects (Filtered) and the target Linear (float4 per
+ * pixel); L1 loss in log(1 + radiance).  loss (host, nullable) receives the
+ * batch's mean loss before the step, after the step completes. */
+ARBOR_API int arbor_denoiser_train_step(arbor_denoiser* d, const uint16_t* features, const float* base, const float* target, int batch, int width, int height, float lr, float* loss);
+/* Denoised Linear (float4 per pixel, .w = 1) of one image:
+ * exp(log(1 + base) + network) - 1. */
+ARBOR_API int arbor_denoiser_infer(arbor_denoiser* d, const uint16_t* features, const float* base, float* denoised, int width, int height);
+/* Forward convolutions on tcgen05 (1, the default) or on mma.sync (0). */
+ARBOR_API int arbor_denoiser_set_backend(arbor_denoiser* d, int tcgen05);
+/* Waits for the stream and reports ARBOR_ERR_TIMEOUT if a tensor-core
+ * convolution gave up waiting for its MMAs since the last check. */
+ARBOR_API int arbor_denoiser_check(arbor_denoiser* d);
+ARBOR_API int arbor_denoiser_destroy(arbor_denoiser* d);
+/* sum = scale * sum + x over `count` floats (progressive sample means). */
+ARBOR_API int arbor_accumulate(float* sum, const float* x, size_t count, float scale, arbor_stream stream);
 
 #ifdef __cplusplus
 }
