@@ -168,18 +168,19 @@ __global__ void __launch_bounds__(128) conv_kernel(ConvArgs a) {
 
 // ------------------------------------------- tcgen05 convolution (sm_100a) --
 // The same 3x3 convolution on the 5th-generation tensor cores: a CTA of 4
-// warps computes 128 consecutive pixels of one output row for all N output
-// channels.  Per chunk of CC input channels it stages the 3 input rows
-// (130 pixels with the halo) and the chunk's weights in shared memory, in the
-// K-major, non-swizzled core-matrix layout the MMA reads (8 rows of 16 bytes
-// per core matrix): a tap's A operand is the staged rows shifted by the tap,
-// so one 128-row descriptor per tap needs no copy.  One thread issues
-// tcgen05.mma (M = 128, N, K = 16, BF16 inputs, FP32 accumulator in TMEM)
-// for 9 taps x CC/16 steps, commits to an mbarrier, and every thread waits
-// (bounded) before the next chunk overwrites the operands.  The epilogue reads
-// the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 =
-// pixels 32w..32w+31 of the tile), applies bias and activation and stores
-// BF16 or FP32.
+// warps computes R consecutive output rows of a 128-pixel column segment for
+// all N output channels.  Per chunk of CC input channels it stages the R + 2
+// input rows (130 pixels with the halo) and the chunk's weights in shared
+// memory with cp.async, in the K-major, non-swizzled core-matrix layout the
+// MMA reads (8 rows of 16 bytes per core matrix): the A operand of output row
+// r and tap (dy, dx) is staged row r + dy shifted by dx, so one 128-row
+// descriptor per (row, tap) needs no copy.  One thread issues tcgen05.mma
+// (M = 128, N, K = 16, BF16 inputs, FP32 accumulators in TMEM, one N-column
+// block per output row) for R rows x 9 taps x CC/16 steps and commits to an
+// mbarrier; every thread waits (bounded) before the next chunk overwrites the
+// operands.  The epilogue reads the accumulators with tcgen05.ld (warp w owns
+// TMEM lanes 32w..32w+31 = pixels 32w..32w+31 of the segment), applies bias
+// and activation and stores BF16 or FP32.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   // start address, leading / stride byte offsets (16-byte units), version 1,
   // no swizzle (layout type 0)
@@ -191,13 +192,10 @@ constexpr uint32_t umma_idesc() {
   // FP32 accumulator, BF16 A and B, both K-major, N >> 3, M = 128 >> 4
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
-template <int N>
-constexpr int tmem_cols() {
-  return N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
-}
-template <int N, int CC>
+constexpr int pow2_cols(int c) { return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512; }
+template <int N, int CC, int R>
 constexpr int conv_tc_smem_bytes() {
-  return (CC / 8) * 3 * 130 * 16 + 9 * (CC / 8) * N * 16 + 16;
+  return (CC / 8) * (R + 2) * 130 * 16 + 9 * (CC / 8) * N * 16 + 16;
 }
 
 // Bounded wait on an mbarrier phase; false when it did not complete.
@@ -213,28 +211,34 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
   }
   return false;
 }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+  // a 16-byte copy, or 16 zero bytes when !valid (src-size 0)
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
 
-template <int N, int CC>
+template <int N, int CC, int R>
 __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
   extern __shared__ __align__(128) uint8_t tc_smem[];
-  constexpr int KU = CC / 8;               // 16-byte K units per chunk
-  constexpr int HALO_B = KU * 3 * 130 * 16;
+  constexpr int KU = CC / 8;                    // 16-byte K units per chunk
+  constexpr int ROWS = R + 2;                   // staged input rows
+  constexpr int HALO_B = KU * ROWS * 130 * 16;
   constexpr int W_B = 9 * KU * N * 16;
-  constexpr uint32_t LBO_A = 3 * 130 * 16;  // next K unit of the halo
-  constexpr uint32_t LBO_B = N * 16;        // next K unit of the weights
-  constexpr int COLS = tmem_cols<N>();
+  constexpr uint32_t LBO_A = ROWS * 130 * 16;   // next K unit of the staged rows
+  constexpr uint32_t LBO_B = N * 16;            // next K unit of the weights
+  constexpr int COLS = pow2_cols(R * N);
   uint8_t* halo = tc_smem;
   uint8_t* wts = tc_smem + HALO_B;
   uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + HALO_B + W_B);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int tiles_x = (a.w + 127) >> 7;
+  const int tiles_x = (a.w + 127) >> 7, rows_y = (a.h + R - 1) / R;
   int t = blockIdx.x;
   const int tx = t % tiles_x;
   t /= tiles_x;
-  const int y = t % a.h, img = t / a.h;
+  const int y0 = (t % rows_y) * R, img = t / rows_y;
   const int x0 = tx * 128;
   const uint32_t bar_a = smem_u32(bar);
+  const uint32_t halo_a = smem_u32(halo), wts_a = smem_u32(wts);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)), "r"(COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
@@ -247,46 +251,48 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = *tmem_slot;
-  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
   uint32_t phase = 0;
   bool ok = true;
   for (int c0 = 0; c0 < a.cin && ok; c0 += CC) {
-    // input rows y-1..y+1, pixels x0-1..x0+128, CC channels: unit (k, r, hx)
-    for (int v = tid; v < 3 * 130 * KU; v += 128) {
+    // input rows y0-1 .. y0+R, pixels x0-1 .. x0+128, CC channels: unit (k, r, hx)
+    for (int v = tid; v < ROWS * 130 * KU; v += 128) {
       const int k = v % KU, rh = v / KU;
       const int r = rh / 130, hx = rh - r * 130;
-      const int gy = y + r - 1, gx = x0 + hx - 1;
-      uint4 val = zero;
-      if (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w)
-        val = *reinterpret_cast<const uint4*>(a.x + ((size_t)(img * a.h + gy) * a.w + gx) * a.cin + c0 + k * 8);
-      *reinterpret_cast<uint4*>(halo + ((k * 3 + r) * 130 + hx) * 16) = val;
+      const int gy = y0 + r - 1, gx = x0 + hx - 1;
+      const bool in = gy >= 0 && gy < a.h && gx >= 0 && gx < a.w;
+      const bf16* src = in ? a.x + ((size_t)(img * a.h + gy) * a.w + gx) * a.cin + c0 + k * 8 : a.x;
+      cp_async16(halo_a + ((k * ROWS + r) * 130 + hx) * 16, src, in);
     }
     // weights: unit (tap, k, n)
     for (int v = tid; v < 9 * KU * N; v += 128) {
       const int k = v % KU, q = v / KU;
       const int tap = q % 9, n = q / 9;
-      uint4 val = zero;
-      if (n < a.cout) val = *reinterpret_cast<const uint4*>(a.wt + ((size_t)n * 9 + tap) * a.cin + c0 + k * 8);
-      *reinterpret_cast<uint4*>(wts + ((tap * KU + k) * N + n) * 16) = val;
+      const bool in = n < a.cout;
+      const bf16* src = in ? a.wt + ((size_t)n * 9 + tap) * a.cin + c0 + k * 8 : a.wt;
+      cp_async16(wts_a + ((tap * KU + k) * N + n) * 16, src, in);
     }
-    // make the generic-proxy stores visible to the tensor cores
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    // make the staged operands visible to the tensor cores
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
       const uint32_t idesc = umma_idesc<N>();
 #pragma unroll 1
-      for (int tap = 0; tap < 9; tap++) {
-        const int dy = tap / 3, dx = tap - dy * 3;
+      for (int r = 0; r < R; r++) {
+#pragma unroll 1
+        for (int tap = 0; tap < 9; tap++) {
+          const int dy = tap / 3, dx = tap - dy * 3;
 #pragma unroll
-        for (int st = 0; st < CC / 16; st++) {
-          const uint64_t da = umma_desc(smem_u32(halo + ((2 * st * 3 + dy) * 130 + dx) * 16), LBO_A, 128);
-          const uint64_t db = umma_desc(smem_u32(wts + ((tap * KU + 2 * st) * N) * 16), LBO_B, 128);
-          const uint32_t acc = (c0 > 0 || tap > 0 || st > 0) ? 1u : 0u;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-              "l"(da), "l"(db), "r"(idesc), "r"(acc));
+          for (int st = 0; st < CC / 16; st++) {
+            const uint64_t da = umma_desc(halo_a + ((2 * st * ROWS + r + dy) * 130 + dx) * 16, LBO_A, 128);
+            const uint64_t db = umma_desc(wts_a + ((tap * KU + 2 * st) * N) * 16, LBO_B, 128);
+            const uint32_t acc = (c0 > 0 || tap > 0 || st > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(r * N)),
+                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+          }
         }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_a) : "memory");
@@ -300,42 +306,45 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
     if (tid == 0) atomicExch(err, 1);
   } else {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-    const int r = warp * 32 + lane;  // this thread's TMEM lane = pixel of the tile
-    const int gx = x0 + r;
-    const size_t p = (size_t)(img * a.h + y) * a.w + gx;
+    const int gx = x0 + warp * 32 + lane;  // this thread's TMEM lane = pixel of the segment
 #pragma unroll 1
-    for (int col = 0; col < N; col += 16) {
-      uint32_t v[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]),
-            "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col));
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      if (gx < a.w) {
-        float f[16];
+    for (int r = 0; r < R; r++) {
+      const int gy = y0 + r;
+      const size_t p = (size_t)(img * a.h + gy) * a.w + gx;
+#pragma unroll 1
+      for (int col = 0; col < N; col += 16) {
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]),
+              "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * N + col)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (gx < a.w && gy < a.h) {
+          float f[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          const int co = col + j;
-          float x = __uint_as_float(v[j]) + (a.bias ? a.bias[co] : 0.0f);
-          if (a.act) x = x > 0.0f ? x : x * kSlope;
-          if (a.mask && !(__bfloat162float(a.mask[p * a.cout + co]) > 0.0f)) x *= kSlope;
-          f[j] = x;
-        }
-        if (a.y_fp32) {
-          float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(a.y) + p * a.cout + col);
-#pragma unroll
-          for (int j = 0; j < 4; j++) o[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
-        } else {
-          uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(a.y) + p * a.cout + col);
-          uint32_t w[8];
-#pragma unroll
-          for (int j = 0; j < 8; j++) {
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
-            w[j] = *reinterpret_cast<const uint32_t*>(&b2);
+          for (int j = 0; j < 16; j++) {
+            const int co = col + j;
+            float x = __uint_as_float(v[j]) + (a.bias ? a.bias[co] : 0.0f);
+            if (a.act) x = x > 0.0f ? x : x * kSlope;
+            if (a.mask && !(__bfloat162float(a.mask[p * a.cout + co]) > 0.0f)) x *= kSlope;
+            f[j] = x;
           }
-          o[0] = make_uint4(w[0], w[1], w[2], w[3]);
-          o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+          if (a.y_fp32) {
+            float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(a.y) + p * a.cout + col);
+#pragma unroll
+            for (int j = 0; j < 4; j++) o[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+          } else {
+            uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(a.y) + p * a.cout + col);
+            uint32_t w[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              const __nv_bfloat162 b2 = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+              w[j] = *reinterpret_cast<const uint32_t*>(&b2);
+            }
+            o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+            o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+          }
         }
       }
     }
@@ -453,82 +462,134 @@ __global__ void bgrad_kernel(const bf16* __restrict__ dy, float* __restrict__ db
 }
 
 // --------------------------------------------------- pooling and concat --
+// All four move 8 channels (16 bytes) per thread; channel counts are
+// multiples of 16.
+__device__ __forceinline__ void unpack8(uint4 v, float (&f)[8]) {
+  const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const float2 t = __bfloat1622float2(b[j]);
+    f[2 * j] = t.x;
+    f[2 * j + 1] = t.y;
+  }
+}
+__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
+  uint4 v;
+  __nv_bfloat162* b = reinterpret_cast<__nv_bfloat162*>(&v);
+#pragma unroll
+  for (int j = 0; j < 4; j++) b[j] = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+  return v;
+}
+
 __global__ void pool_kernel(const bf16* __restrict__ x, bf16* __restrict__ y, int n, int h, int w, int c) {
-  const long total = (long)n * (h / 2) * (w / 2) * c;
+  const int c8 = c / 8;
+  const long total = (long)n * (h / 2) * (w / 2) * c8;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c);
-    long q = i / c;
+    const int ch = (int)(i % c8);
+    long q = i / c8;
     const int X = (int)(q % (w / 2));
     q /= (w / 2);
     const int Y = (int)(q % (h / 2));
     const int img = (int)(q / (h / 2));
-    const size_t b = ((size_t)(img * h + 2 * Y) * w + 2 * X) * c + ch;
-    const float s = __bfloat162float(x[b]) + __bfloat162float(x[b + c]) + __bfloat162float(x[b + (size_t)w * c]) +
-                    __bfloat162float(x[b + (size_t)w * c + c]);
-    y[i] = __float2bfloat16(0.25f * s);
+    const uint4* b = reinterpret_cast<const uint4*>(x + ((size_t)(img * h + 2 * Y) * w + 2 * X) * c) + ch;
+    float s[8], t[8];
+    unpack8(b[0], s);
+    unpack8(b[c8], t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] += t[j];
+    unpack8(b[(size_t)w * c8], t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] += t[j];
+    unpack8(b[(size_t)w * c8 + c8], t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] = 0.25f * (s[j] + t[j]);
+    reinterpret_cast<uint4*>(y)[i] = pack8(s);
   }
 }
 
 // d(skip)[p] = (0.25 * d(pooled)[parent] + dcat[p]) * act'(skip[p])
 __global__ void pool_back_kernel(const bf16* __restrict__ dpool, const bf16* __restrict__ dcat, const bf16* __restrict__ skip,
                                  bf16* __restrict__ dx, int n, int h, int w, int c) {
-  const long total = (long)n * h * w * c;
+  const int c8 = c / 8;
+  const long total = (long)n * h * w * c8;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c);
-    long q = i / c;
+    const int ch = (int)(i % c8);
+    long q = i / c8;
     const int x = (int)(q % w);
     q /= w;
     const int y = (int)(q % h);
     const int img = (int)(q / h);
-    float g = 0.25f * __bfloat162float(dpool[((size_t)(img * (h / 2) + y / 2) * (w / 2) + x / 2) * c + ch]) + __bfloat162float(dcat[i]);
-    if (!(__bfloat162float(skip[i]) > 0.0f)) g *= kSlope;
-    dx[i] = __float2bfloat16(g);
+    float g[8], d[8], m[8];
+    unpack8(reinterpret_cast<const uint4*>(dpool + ((size_t)(img * (h / 2) + y / 2) * (w / 2) + x / 2) * c)[ch], g);
+    unpack8(reinterpret_cast<const uint4*>(dcat)[i], d);
+    unpack8(reinterpret_cast<const uint4*>(skip)[i], m);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      g[j] = 0.25f * g[j] + d[j];
+      if (!(m[j] > 0.0f)) g[j] *= kSlope;
+    }
+    reinterpret_cast<uint4*>(dx)[i] = pack8(g);
   }
 }
 
 // out[p] = concat(skip[p] (cs), low[parent(p)] (cl))
 __global__ void upcat_kernel(const bf16* __restrict__ skip, const bf16* __restrict__ low, bf16* __restrict__ out, int n, int h, int w, int cs,
                              int cl) {
-  const int c = cs + cl;
-  const long total = (long)n * h * w * c;
+  const int c8 = (cs + cl) / 8, s8 = cs / 8, l8 = cl / 8;
+  const long total = (long)n * h * w * c8;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c);
-    const long p = i / c;
-    if (ch < cs) {
-      out[i] = skip[p * cs + ch];
+    const int ch = (int)(i % c8);
+    const long p = i / c8;
+    uint4 v;
+    if (ch < s8) {
+      v = reinterpret_cast<const uint4*>(skip)[p * s8 + ch];
     } else {
       const int x = (int)(p % w);
       const long q = p / w;
       const int y = (int)(q % h);
       const int img = (int)(q / h);
-      out[i] = low[((size_t)(img * (h / 2) + y / 2) * (w / 2) + x / 2) * cl + (ch - cs)];
+      v = reinterpret_cast<const uint4*>(low)[((size_t)(img * (h / 2) + y / 2) * (w / 2) + x / 2) * l8 + (ch - s8)];
     }
+    reinterpret_cast<uint4*>(out)[i] = v;
   }
 }
 
 // dcat -> d(skip part) unmasked (dskip), d(low)[q] = sum of its 4 children's gradients * act'(low[q])
 __global__ void upcat_back_kernel(const bf16* __restrict__ dcat, const bf16* __restrict__ low, bf16* __restrict__ dskip,
                                   bf16* __restrict__ dlow, int n, int h, int w, int cs, int cl) {
-  const int c = cs + cl;
-  const long skip_total = (long)n * h * w * cs;
-  const long low_total = (long)n * (h / 2) * (w / 2) * cl;
+  const int c8 = (cs + cl) / 8, s8 = cs / 8, l8 = cl / 8;
+  const long skip_total = (long)n * h * w * s8;
+  const long low_total = (long)n * (h / 2) * (w / 2) * l8;
+  const uint4* dc = reinterpret_cast<const uint4*>(dcat);
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < skip_total + low_total; i += (long)gridDim.x * blockDim.x) {
     if (i < skip_total) {
-      const long p = i / cs;
-      dskip[i] = dcat[p * c + (i - p * cs)];
+      const long p = i / s8;
+      reinterpret_cast<uint4*>(dskip)[i] = dc[p * c8 + (i - p * s8)];
     } else {
       const long j = i - skip_total;
-      const int ch = (int)(j % cl);
-      long q = j / cl;
+      const int ch = (int)(j % l8);
+      long q = j / l8;
       const int X = (int)(q % (w / 2));
       q /= (w / 2);
       const int Y = (int)(q % (h / 2));
       const int img = (int)(q / (h / 2));
-      const size_t b = ((size_t)(img * h + 2 * Y) * w + 2 * X) * c + cs + ch;
-      float g = __bfloat162float(dcat[b]) + __bfloat162float(dcat[b + c]) + __bfloat162float(dcat[b + (size_t)w * c]) +
-                __bfloat162float(dcat[b + (size_t)w * c + c]);
-      if (!(__bfloat162float(low[j]) > 0.0f)) g *= kSlope;
-      dlow[j] = __float2bfloat16(g);
+      const size_t b = ((size_t)(img * h + 2 * Y) * w + 2 * X) * c8 + s8 + ch;
+      float g[8], t[8], m[8];
+      unpack8(dc[b], g);
+      unpack8(dc[b + c8], t);
+#pragma unroll
+      for (int k = 0; k < 8; k++) g[k] += t[k];
+      unpack8(dc[b + (size_t)w * c8], t);
+#pragma unroll
+      for (int k = 0; k < 8; k++) g[k] += t[k];
+      unpack8(dc[b + (size_t)w * c8 + c8], t);
+      unpack8(reinterpret_cast<const uint4*>(low)[j], m);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        g[k] += t[k];
+        if (!(m[k] > 0.0f)) g[k] *= kSlope;
+      }
+      reinterpret_cast<uint4*>(dlow)[j] = pack8(g);
     }
   }
 }
@@ -661,7 +722,7 @@ int cuda_fail(const char* what, cudaError_t e) {
 
 dim3 ew_grid(long n) {
   long b = (n + 255) / 256;
-  return dim3((unsigned)(b < 4096 ? (b > 0 ? b : 1) : 4096));
+  return dim3((unsigned)(b < 8192 ? (b > 0 ? b : 1) : 8192));
 }
 
 }  // namespace
@@ -750,18 +811,30 @@ int launch_conv(const ConvArgs& a, cudaStream_t s) {
   return check_launch("conv_kernel");
 }
 
-// The forward convolutions on tcgen05 (N = cout up to 128); false when the
-// layer shape has no tcgen05 form here (the caller then uses conv_kernel).
-template <int N, int CC>
+// The forward convolutions on tcgen05 (cout 16..128).  R rows per CTA keep
+// R x N TMEM columns within 256, so two CTAs per SM fit the 512 columns.
+// Shared memory per CTA is padded so that the CTAs one SM can hold never ask
+// for more than its 512 TMEM columns together (an allocation then never
+// waits on another CTA).
+template <int N, int CC, int R>
+constexpr int conv_tc_launch_smem() {
+  constexpr int need = conv_tc_smem_bytes<N, CC, R>();
+  constexpr int floor_b = 228 * 1024 / (512 / pow2_cols(R * N) + 1) + 1024;
+  return need > floor_b ? need : floor_b;
+}
+template <int N, int CC, int R>
 int launch_tc(const ConvArgs& a, int* err, cudaStream_t s) {
+  static_assert(pow2_cols(R * N) <= 256, "TMEM budget");
+  constexpr int smem = conv_tc_launch_smem<N, CC, R>();
+  static_assert(smem <= 227 * 1024, "shared memory per CTA");
   static bool ready = false;
   if (!ready) {
-    if (cudaFuncSetAttribute(conv_tc_kernel<N, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_tc_smem_bytes<N, CC>()) != cudaSuccess)
+    if (cudaFuncSetAttribute(conv_tc_kernel<N, CC, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
       return cuda_fail("cudaFuncSetAttribute (conv_tc)", cudaGetLastError());
     ready = true;
   }
-  const dim3 grid((unsigned)(((a.w + 127) / 128) * a.h * a.n));
-  conv_tc_kernel<N, CC><<<grid, 128, conv_tc_smem_bytes<N, CC>(), s>>>(a, err);
+  const dim3 grid((unsigned)(((a.w + 127) / 128) * ((a.h + R - 1) / R) * a.n));
+  conv_tc_kernel<N, CC, R><<<grid, 128, smem, s>>>(a, err);
   count_launch();
   return check_launch("conv_tc_kernel");
 }
@@ -769,11 +842,11 @@ bool tc_shape(const ConvArgs& a) { return a.cout == 16 || a.cout == 32 || a.cout
 int launch_conv_tc(const ConvArgs& a, int* err, cudaStream_t s) {
   const bool c32 = a.cin % 32 == 0;
   switch (a.cout) {
-    case 16: return c32 ? launch_tc<16, 32>(a, err, s) : launch_tc<16, 16>(a, err, s);
-    case 32: return c32 ? launch_tc<32, 32>(a, err, s) : launch_tc<32, 16>(a, err, s);
-    case 64: return c32 ? launch_tc<64, 32>(a, err, s) : launch_tc<64, 16>(a, err, s);
-    case 96: return c32 ? launch_tc<96, 32>(a, err, s) : launch_tc<96, 16>(a, err, s);
-    default: return c32 ? launch_tc<128, 32>(a, err, s) : launch_tc<128, 16>(a, err, s);
+    case 16: return c32 ? launch_tc<16, 32, 4>(a, err, s) : launch_tc<16, 16, 4>(a, err, s);
+    case 32: return c32 ? launch_tc<32, 32, 4>(a, err, s) : launch_tc<32, 16, 4>(a, err, s);
+    case 64: return c32 ? launch_tc<64, 32, 4>(a, err, s) : launch_tc<64, 16, 4>(a, err, s);
+    case 96: return c32 ? launch_tc<96, 32, 2>(a, err, s) : launch_tc<96, 16, 2>(a, err, s);
+    default: return c32 ? launch_tc<128, 32, 2>(a, err, s) : launch_tc<128, 16, 2>(a, err, s);
   }
 }
 
@@ -836,14 +909,14 @@ int forward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
   };
   auto pool = [&](int src, int dst) {
     const int lv = kAct[src].level;
-    const long n = level_pixels(d, lv + 1, batch, w, h) * kAct[src].channels;
+    const long n = level_pixels(d, lv + 1, batch, w, h) * kAct[src].channels / 8;
     pool_kernel<<<ew_grid(n), 256, 0, s>>>(d->act[src], d->act[dst], batch, h >> lv, w >> lv, kAct[src].channels);
     count_launch();
     return check_launch("pool_kernel");
   };
   auto upcat = [&](int skip, int low, int dst) {
     const int lv = kAct[skip].level;
-    const long n = level_pixels(d, lv, batch, w, h) * kAct[dst].channels;
+    const long n = level_pixels(d, lv, batch, w, h) * kAct[dst].channels / 8;
     upcat_kernel<<<ew_grid(n), 256, 0, s>>>(d->act[skip], d->act[low], d->act[dst], batch, h >> lv, w >> lv, kAct[skip].channels,
                                             kAct[low].channels);
     count_launch();
@@ -883,7 +956,7 @@ int backward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
   auto upcat_back = [&](int cat, int skip_level, int low) {
     const int lv = kAct[cat].level;
     const int cs = kAct[cat].channels - kAct[low].channels, cl = kAct[low].channels;
-    const long n = level_pixels(d, lv, batch, w, h) * cs + level_pixels(d, lv + 1, batch, w, h) * cl;
+    const long n = (level_pixels(d, lv, batch, w, h) * cs + level_pixels(d, lv + 1, batch, w, h) * cl) / 8;
     upcat_back_kernel<<<ew_grid(n), 256, 0, s>>>(d->grad[cat], d->act[low], d->dcat[skip_level], d->grad[low], batch, h >> lv, w >> lv, cs,
                                                  cl);
     count_launch();
@@ -891,7 +964,7 @@ int backward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
   };
   auto pool_back = [&](int pooled, int skip, int skip_level) {
     const int lv = kAct[skip].level;
-    const long n = level_pixels(d, lv, batch, w, h) * kAct[skip].channels;
+    const long n = level_pixels(d, lv, batch, w, h) * kAct[skip].channels / 8;
     pool_back_kernel<<<ew_grid(n), 256, 0, s>>>(d->grad[pooled], d->dcat[skip_level], d->act[skip], d->grad[skip], batch, h >> lv, w >> lv,
                                                 kAct[skip].channels);
     count_launch();

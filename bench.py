@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="arbor", choices=["arbor", "reference"])
-    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "wind", "tree", "batch"])
+    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "wind", "tree", "batch", "denoise"])
     ap.add_argument("--views", type=int, default=64, help="batch workload: views per batch")
     ap.add_argument("--scenes", type=int, default=16, help="batch workload: resident scenes (master seeds)")
     ap.add_argument("--tune-views", type=int, default=8, help="batch workload: views the autotuner times each configuration on")
@@ -653,6 +653,96 @@ def run_reference_batch(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- denoiser --
+# Multiply-accumulates per pixel of the denoiser network (3x3 convolutions;
+# level l runs at 1/4^l of the pixels; the output layer's 3 used channels).
+DENOISER_LAYERS = [(16, 32, 0), (32, 32, 0), (32, 64, 1), (64, 64, 1), (64, 96, 2), (96, 96, 2), (96, 128, 3), (128, 128, 3), (224, 96, 2),
+                   (96, 96, 2), (160, 64, 1), (64, 64, 1), (96, 32, 0), (32, 32, 0), (32, 3, 0)]
+DENOISER_MACS_PER_PIXEL = sum(9 * ci * co / 4 ** lv for ci, co, lv in DENOISER_LAYERS)
+
+
+def run_denoise(args, rank: int, world: int, local_rank: int) -> None:
+    """The learned denoiser at 1920x1080 on a rendered 1-spp forest frame with
+    sun shadows: filterLighting, features and the network per frame (weights
+    untrained: the time does not depend on their values), against
+    filterLighting alone."""
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    import arbor_b200 as ab
+    import workloads
+
+    W, H = 1920, 1080
+    spec = {"workload": "denoise-1080p: learned denoiser (4-level U-Net 32/64/96/128, BF16 tensor cores) on a 1-spp 1920x1080 forest "
+                        "frame with sun shadows, per frame: filterLighting + features + network", "width": W, "height": H}
+    fr = Frames(ab, {**workload_spec("shadows"), "width": W, "height": H}, torch)
+    fr.step(0)
+    Nrm = torch.zeros(W * H * 4, device="cuda")
+    feat = torch.zeros(W * H * 16, dtype=torch.int16, device="cuda")
+    den = torch.zeros(W * H * 4, device="cuda")
+    fr.check(ab.call("arbor_shadeGBuffer", fr.P, fr.Nodes, fr.Order, fr.C, fr.Hit, fr.Lin, fr.Gui, Nrm, W, H))
+    lib = ab.lib()
+    h = ctypes.c_void_p()
+    fr.check(lib.arbor_denoiser_create(ctypes.byref(h), 1, W, H, 7, ab.stream_handle()))
+
+    def frame():
+        fr.check(ab.call("arbor_filterLighting", fr.Lin, fr.Gui, fr.Hit, fr.Fil, fr.C, W, H))
+        fr.check(ab.call("arbor_denoiser_features", fr.Lin, fr.Gui, Nrm, fr.Hit, fr.Fil, W, H, feat))
+        fr.check(lib.arbor_denoiser_infer(h, feat.data_ptr(), fr.Fil.data_ptr(), den.data_ptr(), W, H))
+
+    try:
+        results = {}
+        for backend, name in ((1, "tcgen05"), (0, "mma.sync")):
+            fr.check(lib.arbor_denoiser_set_backend(h, backend))
+            for _ in range(args.warmup):
+                frame()
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            sampler = ClockSampler(physical_gpu(local_rank))
+            sampler.start()
+            time.sleep(0.3)
+            launches0 = ab.launches()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(args.steps):
+                frame()
+            b.record()
+            b.synchronize()
+            fr.check(lib.arbor_denoiser_check(h))
+            results[name] = {"ms": a.elapsed_time(b) / args.steps, "launches": ab.launches() - launches0, "clocks": sampler.stop()}
+        ms_filter = time_kernel(torch, lambda: fr.check(ab.call("arbor_filterLighting", fr.Lin, fr.Gui, fr.Hit, fr.Fil, fr.C, W, H)), 20)
+    finally:
+        lib.arbor_denoiser_destroy(h)
+    peaks = measured_peaks()
+    peak = peaks.get("bf16_tflops")
+    flops = 2.0 * DENOISER_MACS_PER_PIXEL * W * H
+    ms = results["tcgen05"]["ms"]
+    achieved = flops / (ms / 1e3) / 1e12
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    line = {
+        "metric": METRIC, "value": round(float(t.item()), 4), "unit": "ms per 1080p frame (denoiser)", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(float(t.item()), 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16", "data": "synthetic: rendered forest frame (seed 7, walk frame 0, sun shadows); untrained weights",
+        "config": {**spec, "parallelism": f"replicas x{world}",
+                   "l2": "per-frame activations (level 0: 96 channels x 2 M pixels x 2 B = 398 MB) exceed the 126 MB L2"},
+        "phases_ms": {"denoiser_tcgen05": round(results["tcgen05"]["ms"], 4), "denoiser_mma_sync": round(results["mma.sync"]["ms"], 4),
+                      "filterLighting": round(ms_filter, 4)},
+        "roofline": {"kernel": "denoiser network (15 convolutions + elementwise), tcgen05", "bound": "tensor", "achieved": round(achieved, 2),
+                     "peak": peak, "unit": "TFLOP/s", "frac": round(achieved / peak, 4) if peak else None, "traffic": None,
+                     "algorithmic_flops": flops, "macs_per_pixel": round(DENOISER_MACS_PER_PIXEL, 1),
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured, burst)"},
+        "gpu_launches": int(results["tcgen05"]["launches"]),
+        "clocks": results["tcgen05"]["clocks"],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -673,6 +763,8 @@ def main() -> None:
     try:
         if args.workload == "batch":
             run_batch(args, rank, world, local_rank)
+        elif args.workload == "denoise":
+            run_denoise(args, rank, world, local_rank)
         else:
             run_arbor(args, rank, world, local_rank)
     finally:
