@@ -106,6 +106,9 @@ SIGNATURES = {
     "arbor_engine_read_pixels": (_i, [_vp, _vp, ctypes.c_size_t]),
     "arbor_engine_dispose": (_i, [_vp]),
     "arbor_engine_destroy": (_i, [_vp]),
+    "arbor_engine_save_ppm": (_i, [_vp, ctypes.c_char_p]),
+    "arbor_write_ppm": (_i, [ctypes.c_char_p, _vp, _i, _i]),
+    "arbor_write_pfm": (_i, [ctypes.c_char_p, _vp, _i, _i]),
     "arbor_batch_create": (_i, [ctypes.POINTER(_vp), ctypes.POINTER(_i), _i, ctypes.POINTER(BatchView), _i, _vp]),
     "arbor_batch_set_cameras": (_i, [_vp, ctypes.POINTER(_f), _i]),
     "arbor_batch_configure": (_i, [_vp, ctypes.POINTER(BatchConfig)]),

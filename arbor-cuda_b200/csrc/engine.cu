@@ -3,8 +3,10 @@
 // buffer ownership (:22, :40), generate (:27-34), resize (:35-43),
 // frame (:45-53), inspect (:55) and dispose (:57).
 #include <cstdarg>
+#include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "abi_util.h"
 
@@ -385,4 +387,81 @@ extern "C" int arbor_engine_destroy(arbor_engine* e) {
   arbor_engine_dispose(e);
   delete e;
   return ARBOR_OK;
+}
+
+// ------------------------------------------------------------ image files --
+// Binary PPM exactly as the harness writes it (tests/native_harness.cpp:53):
+// "P6\n<w> <h>\n255\n", then R, G, B bytes per pixel (R is Pixels' low byte).
+extern "C" int arbor_write_ppm(const char* path, const uint32_t* pixels, int width, int height) {
+  if (path == nullptr || pixels == nullptr) {
+    set_error("arbor_write_ppm: path and pixels must not be NULL");
+    return ARBOR_ERR_NULL;
+  }
+  if (width <= 0 || height <= 0) {
+    set_error("arbor_write_ppm: %d x %d is not an image", width, height);
+    return ARBOR_ERR_VALUE;
+  }
+  FILE* f = fopen(path, "wb");
+  if (f == nullptr) {
+    set_error("arbor_write_ppm: cannot open %s", path);
+    return ARBOR_ERR_VALUE;
+  }
+  fprintf(f, "P6\n%d %d\n255\n", width, height);
+  std::vector<unsigned char> row((size_t)width * 3);
+  bool ok = true;
+  for (int y = 0; y < height && ok; y++) {
+    for (int x = 0; x < width; x++) {
+      const uint32_t p = pixels[(size_t)y * width + x];
+      row[3 * x] = (unsigned char)(p & 255u);
+      row[3 * x + 1] = (unsigned char)((p >> 8) & 255u);
+      row[3 * x + 2] = (unsigned char)((p >> 16) & 255u);
+    }
+    ok = fwrite(row.data(), 1, row.size(), f) == row.size();
+  }
+  if (fclose(f) != 0) ok = false;
+  if (!ok) {
+    set_error("arbor_write_ppm: write to %s failed", path);
+    return ARBOR_ERR_VALUE;
+  }
+  return ARBOR_OK;
+}
+
+// Portable float map of an RGBA float image (Linear, Guide, Filtered, ...):
+// "PF\n<w> <h>\n-1.0\n", then little-endian float RGB rows, bottom row first.
+extern "C" int arbor_write_pfm(const char* path, const float* rgba, int width, int height) {
+  if (path == nullptr || rgba == nullptr) {
+    set_error("arbor_write_pfm: path and rgba must not be NULL");
+    return ARBOR_ERR_NULL;
+  }
+  if (width <= 0 || height <= 0) {
+    set_error("arbor_write_pfm: %d x %d is not an image", width, height);
+    return ARBOR_ERR_VALUE;
+  }
+  FILE* f = fopen(path, "wb");
+  if (f == nullptr) {
+    set_error("arbor_write_pfm: cannot open %s", path);
+    return ARBOR_ERR_VALUE;
+  }
+  fprintf(f, "PF\n%d %d\n-1.0\n", width, height);
+  std::vector<float> row((size_t)width * 3);
+  bool ok = true;
+  for (int y = height - 1; y >= 0 && ok; y--) {
+    for (int x = 0; x < width; x++)
+      for (int c = 0; c < 3; c++) row[3 * x + c] = rgba[((size_t)y * width + x) * 4 + c];
+    ok = fwrite(row.data(), sizeof(float), row.size(), f) == row.size();
+  }
+  if (fclose(f) != 0) ok = false;
+  if (!ok) {
+    set_error("arbor_write_pfm: write to %s failed", path);
+    return ARBOR_ERR_VALUE;
+  }
+  return ARBOR_OK;
+}
+
+// The engine's current Pixels as a PPM (Renderer::save, native_harness.cpp:53).
+extern "C" int arbor_engine_save_ppm(arbor_engine* e, const char* path) {
+  if (int s = live(e, "arbor_engine_save_ppm")) return s;
+  std::vector<uint32_t> px((size_t)e->width * e->height);
+  if (int s = arbor_engine_read_pixels(e, px.data(), px.size())) return s;
+  return arbor_write_ppm(path, px.data(), e->width, e->height);
 }

@@ -263,6 +263,17 @@ ARBOR_API int arbor_engine_read_pixels(arbor_engine* e, uint32_t* host, size_t c
 ARBOR_API int arbor_engine_dispose(arbor_engine* e);
 /* Disposes (if needed) and frees the handle. */
 ARBOR_API int arbor_engine_destroy(arbor_engine* e);
+/* Writes the engine's Pixels as a binary PPM, as the harness's
+ * Renderer::save does (tests/native_harness.cpp:53). */
+ARBOR_API int arbor_engine_save_ppm(arbor_engine* e, const char* path);
+
+/* Image files from host memory.  PPM: "P6\n<w> <h>\n255\n" then R, G, B
+ * bytes per pixel, R being Pixels' low byte (native_harness.cpp:53).  PFM
+ * (no reference counterpart; float dumps of Linear, Guide, Filtered or a
+ * denoised image): "PF\n<w> <h>\n-1.0\n" then little-endian float RGB rows,
+ * bottom row first. */
+ARBOR_API int arbor_write_ppm(const char* path, const uint32_t* pixels, int width, int height);
+ARBOR_API int arbor_write_pfm(const char* path, const float* rgba, int width, int height);
 
 
 /* ---------------------------------------------------------------------------

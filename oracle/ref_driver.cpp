@@ -205,6 +205,14 @@ EXPORT void oracle_harnessBuild(int seed, float* B, float* P, unsigned* Keys, un
   std::copy(r.order.begin(), r.order.end(), Order);
   std::copy(r.nodes.begin(), r.nodes.end(), Nodes);
 }
+// The harness's own PPM writer (Renderer::save, native_harness.cpp:53) on the
+// given pixels, to pin the library's PPM output to it byte for byte.
+EXPORT void oracle_harnessSave(const unsigned* pixels, int width, int height, const char* path) {
+  Renderer r(1788);
+  r.resize(width, height);
+  std::copy(pixels, pixels + (size_t)width * height, r.pixels.begin());
+  r.save(path);
+}
 EXPORT void oracle_exhaustiveRay(const float* P, const float* ro, const float* rd, float cone, float* out) {
   float3 o = make_float3(ro[0], ro[1], ro[2]), d = make_float3(rd[0], rd[1], rd[2]);
   float nearest = FAR; int winner = -1;

@@ -149,3 +149,37 @@ def test_batch_rejections_without_device(lib):
     assert lib.arbor_batch_create(ctypes.byref(h), seeds, 2, views, 2, None) == ab.ERR_NO_DEVICE
     assert lib.arbor_batch_render(None) == ab.ERR_NULL
     assert lib.arbor_batch_destroy(None) == ab.OK
+
+
+def test_image_files(lib, tmp_path):
+    """PPM bytes equal the reference harness's own writer (Renderer::save,
+    tests/native_harness.cpp:53) when its build is present; PFM layout."""
+    import ctypes
+
+    import numpy as np
+
+    w, h = 7, 3
+    px = (np.arange(w * h, dtype=np.uint32) * 2654435761).astype(np.uint32) | np.uint32(0xFF000000)
+    ppm = tmp_path / "a.ppm"
+    assert lib.arbor_write_ppm(str(ppm).encode(), px.ctypes.data, w, h) == ab.OK
+    data = ppm.read_bytes()
+    rgb = np.stack([px & 255, (px >> 8) & 255, (px >> 16) & 255], 1).astype(np.uint8).tobytes()
+    assert data == f"P6\n{w} {h}\n255\n".encode() + rgb
+    ref_so = os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "libarbor_ref.so")
+    if os.path.exists(ref_so):
+        ref = ctypes.CDLL(ref_so)
+        if hasattr(ref, "oracle_harnessSave"):
+            ref.oracle_harnessSave.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
+            out = tmp_path / "ref.ppm"
+            ref.oracle_harnessSave(px.ctypes.data, w, h, str(out).encode())
+            assert out.read_bytes() == data
+    img = np.random.default_rng(0).random(w * h * 4).astype(np.float32)
+    pfm = tmp_path / "a.pfm"
+    assert lib.arbor_write_pfm(str(pfm).encode(), img.ctypes.data, w, h) == ab.OK
+    raw = pfm.read_bytes()
+    head = f"PF\n{w} {h}\n-1.0\n".encode()
+    assert raw.startswith(head)
+    body = np.frombuffer(raw[len(head):], "<f4").reshape(h, w, 3)
+    assert np.array_equal(body[::-1], img.reshape(h, w, 4)[..., :3])
+    assert lib.arbor_write_ppm(None, px.ctypes.data, w, h) == ab.ERR_NULL
+    assert lib.arbor_write_ppm(str(ppm).encode(), px.ctypes.data, 0, h) == ab.ERR_VALUE

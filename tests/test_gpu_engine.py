@@ -106,3 +106,20 @@ def test_timing_reports_phases(engine):
     engine.frame(1 / 60)
     info = engine.inspect()
     assert info.ms_visibility > 0 and info.ms_lighting > 0 and info.ms_resolve > 0
+
+
+def test_save_ppm_matches_pixels(cuda, tmp_path):
+    """arbor_engine_save_ppm writes the frame the engine holds, in the
+    harness's PPM format (tests/native_harness.cpp:53)."""
+    e = ab.Engine(320, 192, seed=1788)
+    try:
+        e.frame(1 / 60)
+        info = e.inspect()
+        px = np.zeros(info.width * info.height, np.uint32)
+        e.read_pixels_into(px.ctypes.data, px.size)
+        path = tmp_path / "frame.ppm"
+        ab.check(ab.lib().arbor_engine_save_ppm(e.handle, str(path).encode()))
+        rgb = np.stack([px & 255, (px >> 8) & 255, (px >> 16) & 255], 1).astype(np.uint8).tobytes()
+        assert path.read_bytes() == f"P6\n{info.width} {info.height}\n255\n".encode() + rgb
+    finally:
+        e.close()
