@@ -171,14 +171,15 @@ __global__ void __launch_bounds__(128) conv_kernel(ConvArgs a) {
 // warps computes R consecutive output rows of a 128-pixel column segment for
 // all N output channels.  Per chunk of CC input channels it stages the R + 2
 // input rows (130 pixels with the halo) and the chunk's weights in shared
-// memory with cp.async, in the K-major, non-swizzled core-matrix layout the
+// memory with cp.async (two stage buffers: chunk c + 1 loads while chunk c's
+// MMAs run), in the K-major, non-swizzled core-matrix layout the
 // MMA reads (8 rows of 16 bytes per core matrix): the A operand of output row
 // r and tap (dy, dx) is staged row r + dy shifted by dx, so one 128-row
 // descriptor per (row, tap) needs no copy.  One thread issues tcgen05.mma
 // (M = 128, N, K = 16, BF16 inputs, FP32 accumulators in TMEM, one N-column
 // block per output row) for R rows x 9 taps x CC/16 steps and commits to an
-// mbarrier; every thread waits (bounded) before the next chunk overwrites the
-// operands.  The epilogue reads the accumulators with tcgen05.ld (warp w owns
+// mbarrier; every thread waits (bounded) for a chunk's MMAs before its stage
+// buffer is refilled.  The epilogue reads the accumulators with tcgen05.ld (warp w owns
 // TMEM lanes 32w..32w+31 = pixels 32w..32w+31 of the segment), applies bias
 // and activation and stores BF16 or FP32.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -194,8 +195,12 @@ constexpr uint32_t umma_idesc() {
 }
 constexpr int pow2_cols(int c) { return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512; }
 template <int N, int CC, int R>
+constexpr int conv_tc_stage_bytes() {
+  return (CC / 8) * (R + 2) * 130 * 16 + 9 * (CC / 8) * N * 16;
+}
+template <int N, int CC, int R>
 constexpr int conv_tc_smem_bytes() {
-  return (CC / 8) * (R + 2) * 130 * 16 + 9 * (CC / 8) * N * 16 + 16;
+  return 2 * conv_tc_stage_bytes<N, CC, R>() + N * 4 + 16;  // two stages, biases, mbarrier, TMEM slot
 }
 
 // Bounded wait on an mbarrier phase; false when it did not complete.
@@ -222,13 +227,12 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
   constexpr int KU = CC / 8;                    // 16-byte K units per chunk
   constexpr int ROWS = R + 2;                   // staged input rows
   constexpr int HALO_B = KU * ROWS * 130 * 16;
-  constexpr int W_B = 9 * KU * N * 16;
+  constexpr int STAGE_B = conv_tc_stage_bytes<N, CC, R>();
   constexpr uint32_t LBO_A = ROWS * 130 * 16;   // next K unit of the staged rows
   constexpr uint32_t LBO_B = N * 16;            // next K unit of the weights
   constexpr int COLS = pow2_cols(R * N);
-  uint8_t* halo = tc_smem;
-  uint8_t* wts = tc_smem + HALO_B;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + HALO_B + W_B);
+  float* bias_s = reinterpret_cast<float*>(tc_smem + 2 * STAGE_B);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(bias_s + N);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tiles_x = (a.w + 127) >> 7, rows_y = (a.h + R - 1) / R;
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
   const int y0 = (t % rows_y) * R, img = t / rows_y;
   const int x0 = tx * 128;
   const uint32_t bar_a = smem_u32(bar);
-  const uint32_t halo_a = smem_u32(halo), wts_a = smem_u32(wts);
+  const uint32_t smem_a = smem_u32(tc_smem);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)), "r"(COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
@@ -247,14 +251,10 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_a), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
-  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-  const uint32_t tmem = *tmem_slot;
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int c0 = 0; c0 < a.cin && ok; c0 += CC) {
-    // input rows y0-1 .. y0+R, pixels x0-1 .. x0+128, CC channels: unit (k, r, hx)
+  for (int i = tid; i < N; i += 128) bias_s[i] = a.bias && i < a.cout ? a.bias[i] : 0.0f;
+  // Stage the operands of the chunk starting at channel c0 into stage buffer sb.
+  auto stage = [&](int c0, int sb) {
+    const uint32_t halo_a = smem_a + sb * STAGE_B, wts_a = halo_a + HALO_B;
     for (int v = tid; v < ROWS * 130 * KU; v += 128) {
       const int k = v % KU, rh = v / KU;
       const int r = rh / 130, hx = rh - r * 130;
@@ -263,7 +263,6 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
       const bf16* src = in ? a.x + ((size_t)(img * a.h + gy) * a.w + gx) * a.cin + c0 + k * 8 : a.x;
       cp_async16(halo_a + ((k * ROWS + r) * 130 + hx) * 16, src, in);
     }
-    // weights: unit (tap, k, n)
     for (int v = tid; v < 9 * KU * N; v += 128) {
       const int k = v % KU, q = v / KU;
       const int tap = q % 9, n = q / 9;
@@ -271,37 +270,57 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
       const bf16* src = in ? a.wt + ((size_t)n * 9 + tap) * a.cin + c0 + k * 8 : a.wt;
       cp_async16(wts_a + ((tap * KU + k) * N + n) * 16, src, in);
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  const int chunks = a.cin / CC;
+  bool ok = true;
+  stage(0, 0);
+  for (int c = 0; c < chunks && ok; c++) {
+    // The chunk c-1 MMAs must be done before their buffer takes chunk c+1.
+    if (c > 0) ok = __syncthreads_and(mbar_wait(bar_a, (uint32_t)((c - 1) & 1)) ? 1 : 0) != 0;
+    if (!ok) break;
+    if (c + 1 < chunks) {
+      stage((c + 1) * CC, (c + 1) & 1);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // chunk c's copies are in
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
     // make the staged operands visible to the tensor cores
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
       const uint32_t idesc = umma_idesc<N>();
-#pragma unroll 1
+      const uint32_t halo_a = smem_a + (c & 1) * STAGE_B, wts_a = halo_a + HALO_B;
+      // descriptors advance by address only (16-byte units in the low bits)
+      const uint64_t da0 = umma_desc(halo_a, LBO_A, 128), db0 = umma_desc(wts_a, LBO_B, 128);
+      uint32_t acc = c > 0 ? 1u : 0u;
+#pragma unroll
       for (int r = 0; r < R; r++) {
-#pragma unroll 1
+#pragma unroll
         for (int tap = 0; tap < 9; tap++) {
-          const int dy = tap / 3, dx = tap - dy * 3;
 #pragma unroll
           for (int st = 0; st < CC / 16; st++) {
-            const uint64_t da = umma_desc(halo_a + ((2 * st * ROWS + r + dy) * 130 + dx) * 16, LBO_A, 128);
-            const uint64_t db = umma_desc(wts_a + ((tap * KU + 2 * st) * N) * 16, LBO_B, 128);
-            const uint32_t acc = (c0 > 0 || tap > 0 || st > 0) ? 1u : 0u;
+            const uint64_t da = da0 + (uint64_t)((((2 * st * ROWS + r + tap / 3) * 130 + tap % 3) * 16) >> 4);
+            const uint64_t db = db0 + (uint64_t)(((tap * KU + 2 * st) * N * 16) >> 4);
+            const uint32_t acc_rt = (tap > 0 || st > 0) ? 1u : acc;
             asm volatile(
                 "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(r * N)),
-                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                "l"(da), "l"(db), "r"(idesc), "r"(acc_rt));
           }
         }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_a) : "memory");
     }
-    // every thread waits for the MMAs (bounded); the barrier makes the
-    // outcome uniform, so all threads leave the loop together
-    ok = __syncthreads_and(mbar_wait(bar_a, phase) ? 1 : 0) != 0;
-    phase ^= 1u;
   }
+  // the last chunk's MMAs (bounded, uniform outcome)
+  if (ok) ok = __syncthreads_and(mbar_wait(bar_a, (uint32_t)((chunks - 1) & 1)) ? 1 : 0) != 0;
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
   } else {
@@ -325,7 +344,7 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
 #pragma unroll
           for (int j = 0; j < 16; j++) {
             const int co = col + j;
-            float x = __uint_as_float(v[j]) + (a.bias ? a.bias[co] : 0.0f);
+            float x = __uint_as_float(v[j]) + bias_s[co];
             if (a.act) x = x > 0.0f ? x : x * kSlope;
             if (a.mask && !(__bfloat162float(a.mask[p * a.cout + co]) > 0.0f)) x *= kSlope;
             f[j] = x;
@@ -840,13 +859,12 @@ int launch_tc(const ConvArgs& a, int* err, cudaStream_t s) {
 }
 bool tc_shape(const ConvArgs& a) { return a.cout == 16 || a.cout == 32 || a.cout == 64 || a.cout == 96 || a.cout == 128; }
 int launch_conv_tc(const ConvArgs& a, int* err, cudaStream_t s) {
-  const bool c32 = a.cin % 32 == 0;
   switch (a.cout) {
-    case 16: return c32 ? launch_tc<16, 32, 4>(a, err, s) : launch_tc<16, 16, 4>(a, err, s);
-    case 32: return c32 ? launch_tc<32, 32, 4>(a, err, s) : launch_tc<32, 16, 4>(a, err, s);
-    case 64: return c32 ? launch_tc<64, 32, 4>(a, err, s) : launch_tc<64, 16, 4>(a, err, s);
-    case 96: return c32 ? launch_tc<96, 32, 2>(a, err, s) : launch_tc<96, 16, 2>(a, err, s);
-    default: return c32 ? launch_tc<128, 32, 2>(a, err, s) : launch_tc<128, 16, 2>(a, err, s);
+    case 16: return launch_tc<16, 16, 8>(a, err, s);
+    case 32: return launch_tc<32, 16, 8>(a, err, s);
+    case 64: return launch_tc<64, 16, 4>(a, err, s);
+    case 96: return launch_tc<96, 16, 2>(a, err, s);
+    default: return launch_tc<128, 16, 2>(a, err, s);
   }
 }
 
