@@ -22,8 +22,10 @@
 //                   previous layer's activation derivative in its epilogue.
 //   wgrad_kernel    weight gradients: a GEMM over pixels of the output
 //                   gradient and the shifted input, FP32 atomics per CTA
-//   pool / upcat    2x2 average pooling, nearest upsampling + skip concat,
-//                   and their backward passes with activation derivatives
+//   pool / upcat    2x2 average pooling and its backward pass; the backward
+//                   pass of nearest upsampling + skip concatenation (the
+//                   forward concatenation is read in place by the decoder
+//                   convolutions), with activation derivatives
 //   loss, adam, features, output: elementwise
 #include <cuda_bf16.h>
 
@@ -68,7 +70,19 @@ struct ConvArgs {
   int cin, cout, n, h, w;
   int act;            // leaky ReLU on the output
   int y_fp32;
+  // Optional second input: channels [cs, cin) are x2 (cin - cs channels) at
+  // half resolution, upsampled by nearest neighbour, and x holds channels
+  // [0, cs) - the decoder's concatenation, read without being stored.
+  const bf16* x2;
+  int cs;
 };
+
+// Address of input channels [c, c + 8) of pixel (img, gy, gx).
+__device__ __forceinline__ const bf16* conv_in(const bf16* x, const bf16* x2, int cin, int cs, int h, int w, int img, int gy, int gx, int c) {
+  if (x2 == nullptr) return x + ((size_t)(img * h + gy) * w + gx) * cin + c;
+  if (c < cs) return x + ((size_t)(img * h + gy) * w + gx) * cs + c;
+  return x2 + ((size_t)(img * (h >> 1) + (gy >> 1)) * (w >> 1) + (gx >> 1)) * (cin - cs) + (c - cs);
+}
 
 // smem layout of one stage: halo [100][KC+8], weights [NT*8*9][KC+8] (bf16)
 template <int KC, int NT>
@@ -99,7 +113,7 @@ __global__ void __launch_bounds__(128) conv_kernel(ConvArgs a) {
       const int gy = ty * 8 + hy - 1, gx = tx * 8 + hx - 1;
       uint4 val = zero;
       if (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w)
-        val = *reinterpret_cast<const uint4*>(a.x + ((size_t)(img * a.h + gy) * a.w + gx) * a.cin + c0 + part * 8);
+        val = *reinterpret_cast<const uint4*>(conv_in(a.x, a.x2, a.cin, a.cs, a.h, a.w, img, gy, gx, c0 + part * 8));
       *reinterpret_cast<uint4*>(halo + pix * RS + part * 8) = val;
     }
     // weights: NT*8 output channels x 9 taps x KC input channels
@@ -260,7 +274,7 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
       const int r = rh / 130, hx = rh - r * 130;
       const int gy = y0 + r - 1, gx = x0 + hx - 1;
       const bool in = gy >= 0 && gy < a.h && gx >= 0 && gx < a.w;
-      const bf16* src = in ? a.x + ((size_t)(img * a.h + gy) * a.w + gx) * a.cin + c0 + k * 8 : a.x;
+      const bf16* src = in ? conv_in(a.x, a.x2, a.cin, a.cs, a.h, a.w, img, gy, gx, c0 + k * 8) : a.x;
       cp_async16(halo_a + ((k * ROWS + r) * 130 + hx) * 16, src, in);
     }
     for (int v = tid; v < 9 * KU * N; v += 128) {
@@ -379,10 +393,12 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
 // one tap, over a contiguous range of pixels, 32 at a time.
 struct WgradArgs {
   const bf16* dy;  // NHWC, cout channels
-  const bf16* x;   // NHWC, cin channels
+  const bf16* x;   // NHWC, cin channels (or cs channels with x2, as ConvArgs)
   float* dw;       // [cout][9][cin], accumulated
   int cin, cout, n, h, w;
   int pixels_per_cta;
+  const bf16* x2;
+  int cs;
 };
 
 template <int CI>
@@ -424,7 +440,7 @@ __global__ void __launch_bounds__(128) wgrad_kernel(WgradArgs a) {
         const int rem = (int)(p - (long)img * a.h * a.w);
         const int y = rem / a.w + dy, xx = rem % a.w + dx;
         if (y >= 0 && y < a.h && xx >= 0 && xx < a.w)
-          val = *reinterpret_cast<const uint4*>(a.x + ((size_t)(img * a.h + y) * a.w + xx) * a.cin + ci0 + part * 8);
+          val = *reinterpret_cast<const uint4*>(conv_in(a.x, a.x2, a.cin, a.cs, a.h, a.w, img, y, xx, ci0 + part * 8));
       }
       *reinterpret_cast<uint4*>(xs + r * XS + part * 8) = val;
     }
@@ -548,28 +564,6 @@ __global__ void pool_back_kernel(const bf16* __restrict__ dpool, const bf16* __r
       if (!(m[j] > 0.0f)) g[j] *= kSlope;
     }
     reinterpret_cast<uint4*>(dx)[i] = pack8(g);
-  }
-}
-
-// out[p] = concat(skip[p] (cs), low[parent(p)] (cl))
-__global__ void upcat_kernel(const bf16* __restrict__ skip, const bf16* __restrict__ low, bf16* __restrict__ out, int n, int h, int w, int cs,
-                             int cl) {
-  const int c8 = (cs + cl) / 8, s8 = cs / 8, l8 = cl / 8;
-  const long total = (long)n * h * w * c8;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int ch = (int)(i % c8);
-    const long p = i / c8;
-    uint4 v;
-    if (ch < s8) {
-      v = reinterpret_cast<const uint4*>(skip)[p * s8 + ch];
-    } else {
-      const int x = (int)(p % w);
-      const long q = p / w;
-      const int y = (int)(q % h);
-      const int img = (int)(q / h);
-      v = reinterpret_cast<const uint4*>(low)[((size_t)(img * (h / 2) + y / 2) * (w / 2) + x / 2) * l8 + (ch - s8)];
-    }
-    reinterpret_cast<uint4*>(out)[i] = v;
   }
 }
 
@@ -775,6 +769,9 @@ constexpr ActSpec kAct[kActs] = {{0, kFeat}, {0, 32}, {0, 32}, {1, 32}, {1, 64},
 // input and output tensor of each convolution (the output layer writes `out`)
 constexpr int kIn[kLayers] = {aF, aE0a, aP1, aE1a, aP2, aE2a, aP3, aB3a, aC2, aD2a, aC1, aD1a, aC0, aD0a, aD0};
 constexpr int kOut[kLayers] = {aE0a, aE0, aE1a, aE1, aE2a, aE2, aB3a, aB3, aD2a, aD2, aD1a, aD1, aD0a, aD0, -1};
+// decoder inputs read as (skip, level below) without storing the concatenation
+constexpr int kCat[kLayers][2] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}, {aE2, aB3}, {-1, -1},
+                                  {aE1, aD2}, {-1, -1}, {aE0, aD1}, {-1, -1}, {-1, -1}};
 }  // namespace
 
 struct arbor_denoiser {
@@ -868,8 +865,8 @@ int launch_conv_tc(const ConvArgs& a, int* err, cudaStream_t s) {
   }
 }
 
-int launch_wgrad(const bf16* dy, const bf16* x, float* dw, int cin, int cout, int n, int h, int w, cudaStream_t s) {
-  WgradArgs a{dy, x, dw, cin, cout, n, h, w, 0};
+int launch_wgrad(const bf16* dy, const bf16* x, const bf16* x2, int cs, float* dw, int cin, int cout, int n, int h, int w, cudaStream_t s) {
+  WgradArgs a{dy, x, dw, cin, cout, n, h, w, 0, x2, cs};
   const long pixels = (long)n * h * w;
   const int ci_tile = cin % 32 == 0 ? 32 : 16;
   const int base = ((cout + 63) / 64) * 9 * (cin / ci_tile);
@@ -922,7 +919,12 @@ int forward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
     const int lv = kAct[kIn[l]].level;
     ConvArgs a{in[kIn[l]], d->wf + d->wf_off[l], d->p + L.boff,
                kOut[l] < 0 ? (void*)d->out : (void*)d->act[kOut[l]], nullptr, L.cin, L.cout, batch, h >> lv, w >> lv, kSpec[l][2],
-               kOut[l] < 0 ? 1 : 0};
+               kOut[l] < 0 ? 1 : 0, nullptr, 0};
+    if (kCat[l][0] >= 0) {  // a decoder input: read the skip and the upsampled level below in place
+      a.x = d->act[kCat[l][0]];
+      a.x2 = d->act[kCat[l][1]];
+      a.cs = kAct[kCat[l][0]].channels;
+    }
     return d->tc && tc_shape(a) ? launch_conv_tc(a, d->err, s) : launch_conv(a, s);
   };
   auto pool = [&](int src, int dst) {
@@ -932,19 +934,10 @@ int forward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
     count_launch();
     return check_launch("pool_kernel");
   };
-  auto upcat = [&](int skip, int low, int dst) {
-    const int lv = kAct[skip].level;
-    const long n = level_pixels(d, lv, batch, w, h) * kAct[dst].channels / 8;
-    upcat_kernel<<<ew_grid(n), 256, 0, s>>>(d->act[skip], d->act[low], d->act[dst], batch, h >> lv, w >> lv, kAct[skip].channels,
-                                            kAct[low].channels);
-    count_launch();
-    return check_launch("upcat_kernel");
-  };
   int st;
   if ((st = conv(0)) || (st = conv(1)) || (st = pool(aE0, aP1)) || (st = conv(2)) || (st = conv(3)) || (st = pool(aE1, aP2)) ||
-      (st = conv(4)) || (st = conv(5)) || (st = pool(aE2, aP3)) || (st = conv(6)) || (st = conv(7)) || (st = upcat(aE2, aB3, aC2)) ||
-      (st = conv(8)) || (st = conv(9)) || (st = upcat(aE1, aD2, aC1)) || (st = conv(10)) || (st = conv(11)) ||
-      (st = upcat(aE0, aD1, aC0)) || (st = conv(12)) || (st = conv(13)) || (st = conv(14)))
+      (st = conv(4)) || (st = conv(5)) || (st = pool(aE2, aP3)) || (st = conv(6)) || (st = conv(7)) || (st = conv(8)) ||
+      (st = conv(9)) || (st = conv(10)) || (st = conv(11)) || (st = conv(12)) || (st = conv(13)) || (st = conv(14)))
     return st;
   return ARBOR_OK;
 }
@@ -957,7 +950,10 @@ int backward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
   auto wgrad = [&](int l, const bf16* dy) {
     const LayerParams& L = d->layer[l];
     const int lv = kAct[kIn[l]].level;
-    if (int st = launch_wgrad(dy, x_of(l), d->g + L.woff, L.cin, L.cout, batch, h >> lv, w >> lv, s)) return st;
+    const bool cat = kCat[l][0] >= 0;
+    if (int st = launch_wgrad(dy, cat ? d->act[kCat[l][0]] : x_of(l), cat ? d->act[kCat[l][1]] : nullptr, cat ? kAct[kCat[l][0]].channels : 0,
+                              d->g + L.woff, L.cin, L.cout, batch, h >> lv, w >> lv, s))
+      return st;
     const long px = level_pixels(d, lv, batch, w, h);
     bgrad_kernel<<<(unsigned)std::min<long>(1184, (px * L.cout + 255) / 256 + 1), 256, 0, s>>>(dy, d->g + L.boff, L.cout, px);
     count_launch();
@@ -968,7 +964,8 @@ int backward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
   auto dgrad = [&](int l, const bf16* dy, bf16* dx, int mask_act) {
     const LayerParams& L = d->layer[l];
     const int lv = kAct[kIn[l]].level;
-    ConvArgs a{dy, d->wb + d->wf_off[l], nullptr, dx, mask_act >= 0 ? d->act[mask_act] : nullptr, L.cout, L.cin, batch, h >> lv, w >> lv, 0, 0};
+    ConvArgs a{dy, d->wb + d->wf_off[l], nullptr, dx, mask_act >= 0 ? d->act[mask_act] : nullptr, L.cout, L.cin, batch, h >> lv, w >> lv, 0, 0,
+               nullptr, 0};
     return launch_conv(a, s);
   };
   auto upcat_back = [&](int cat, int skip_level, int low) {
@@ -1089,7 +1086,8 @@ extern "C" int arbor_denoiser_create(arbor_denoiser** out, int max_batch, int ma
   const long px0 = (long)max_batch * max_width * max_height;
   for (int k = 0; k < kActs; k++) {
     const size_t bytes = (size_t)(px0 >> (2 * kAct[k].level)) * kAct[k].channels * 2;
-    if (k != aF && !alloc((void**)&d->act[k], bytes)) return fail(cuda_fail("cudaMalloc (denoiser activations)", ce));
+    const bool concat = k == aC0 || k == aC1 || k == aC2;  // read in place by the decoder convolutions, never stored
+    if (k != aF && !concat && !alloc((void**)&d->act[k], bytes)) return fail(cuda_fail("cudaMalloc (denoiser activations)", ce));
     if (!alloc((void**)&d->grad[k], bytes)) return fail(cuda_fail("cudaMalloc (denoiser gradients)", ce));
   }
   const int skips[3] = {aE0, aE1, aE2};

@@ -132,43 +132,48 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
       b.miscJob[om++] = (short)q;
   }
   __syncwarp();
-  // leaf clips; the clips that pass queue a Newton solve
+  // Leaf clips, 32 jobs at a time while fewer than 32 Newton solves are
+  // pending; the clips that pass queue a Newton solve; a full pass of 32
+  // solves (or the rest, once every clip is done) runs at the single call site
+  // of leaf_newton below.
   int nN = 0;
-  for (int base = 0; base < totL; base += 32) {
-    int j = base + lane;
-    bool solve = false;
-    LeafSolve ls;
-    int q = 0;
-    if (j < totL) {
-      q = b.leafJob[j];
-      int owner = q / WB::kQ;
-      float4 o = b.rayO[owner], d = b.rayD[owner];
-      solve = leaf_clip(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls);
-      if (!solve) b.res[q] = ls.best;
+  for (int base = 0;;) {
+    if (base < totL && nN < 32) {
+      int j = base + lane;
+      bool solve = false;
+      LeafSolve ls;
+      int q = 0;
+      if (j < totL) {
+        q = b.leafJob[j];
+        int owner = q / WB::kQ;
+        float4 o = b.rayO[owner], d = b.rayD[owner];
+        solve = leaf_clip(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls);
+        if (!solve) b.res[q] = ls.best;
+      }
+      unsigned m = __ballot_sync(full, solve);
+      if (solve) {
+        int pos = nN + __popc(m & lt);
+        b.solve[pos] = ls;
+        b.solveJob[pos] = (short)q;
+      }
+      nN += __popc(m);
+      base += 32;
+      __syncwarp();
+      continue;
     }
-    unsigned m = __ballot_sync(full, solve);
-    if (solve) {
-      int pos = nN + __popc(m & lt);
-      b.solve[pos] = ls;
-      b.solveJob[pos] = (short)q;
-    }
-    nN += __popc(m);
-    __syncwarp();
-    if (nN >= 32) {  // a full pass of Newton solves
+    if (nN == 0) break;
+    const int run = nN < 32 ? nN : 32;
+    if (lane < run) {
       int qn = b.solveJob[lane];
       b.res[qn] = leaf_newton(b.solve[lane], b.fp[qn]);
-      __syncwarp();
-      if (lane < nN - 32) {
-        b.solve[lane] = b.solve[32 + lane];
-        b.solveJob[lane] = b.solveJob[32 + lane];
-      }
-      nN -= 32;
-      __syncwarp();
     }
-  }
-  if (lane < nN) {
-    int qn = b.solveJob[lane];
-    b.res[qn] = leaf_newton(b.solve[lane], b.fp[qn]);
+    __syncwarp();
+    if (lane < nN - run) {
+      b.solve[lane] = b.solve[run + lane];
+      b.solveJob[lane] = b.solveJob[run + lane];
+    }
+    nN -= run;
+    __syncwarp();
   }
   // wood tests (tube + SDF march)
   for (int base = 0; base < totW; base += 32) {
