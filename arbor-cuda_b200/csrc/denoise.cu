@@ -387,6 +387,164 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs a, int* err) {
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(COLS));
 }
 
+// Row-streaming form for the layers whose weights fit in shared memory
+// with a 5-row input ring: a CTA keeps all 9 x CIN x N weights resident and
+// walks down its rows of one 128-pixel column segment.  Per output row y it
+// starts loading input row y + 2 (all CIN channels, cp.async) into the ring,
+// waits for row y + 1, one thread issues the row's 9 x CIN/16 MMAs into one
+// of two TMEM accumulators, and the 4 warps run the previous row's epilogue
+// while those MMAs execute; each input row is read from memory once per
+// segment.
+template <int N, int CIN>
+constexpr int conv_row_smem_bytes() {
+  return 9 * (CIN / 8) * N * 16 + 5 * (CIN / 8) * 130 * 16 + N * 4 + 32;
+}
+
+template <int N, int CIN>
+__global__ void __launch_bounds__(128) conv_row_kernel(ConvArgs a, int rows_per_cta, int* err) {
+  extern __shared__ __align__(128) uint8_t rs_smem[];
+  constexpr int KU = CIN / 8;
+  constexpr int W_B = 9 * KU * N * 16;
+  constexpr int SLOT_B = KU * 130 * 16;        // one staged input row
+  constexpr uint32_t LBO_A = 130 * 16;         // next K unit within a staged row
+  constexpr uint32_t LBO_B = N * 16;           // next K unit of the weights
+  constexpr int COLS = pow2_cols(2 * N);
+  const uint32_t smem_a = smem_u32(rs_smem);
+  const uint32_t wts_a = smem_a, ring_a = smem_a + W_B;
+  float* bias_s = reinterpret_cast<float*>(rs_smem + W_B + 5 * SLOT_B);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(bias_s + N);  // two mbarriers, one per accumulator
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles_x = (a.w + 127) >> 7, groups = (a.h + rows_per_cta - 1) / rows_per_cta;
+  int t = blockIdx.x;
+  const int tx = t % tiles_x;
+  t /= tiles_x;
+  const int y_begin = (t % groups) * rows_per_cta, img = t / groups;
+  const int y_end = y_begin + rows_per_cta < a.h ? y_begin + rows_per_cta : a.h;
+  const int x0 = tx * 128;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)), "r"(COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar + 1)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+  for (int i = tid; i < N; i += 128) bias_s[i] = a.bias && i < a.cout ? a.bias[i] : 0.0f;
+  // weights: unit (tap, k, n)
+  for (int v = tid; v < 9 * KU * N; v += 128) {
+    const int k = v % KU, q = v / KU;
+    const int tap = q % 9, n = q / 9;
+    const bool in = n < a.cout;
+    cp_async16(wts_a + ((tap * KU + k) * N + n) * 16, in ? a.wt + ((size_t)n * 9 + tap) * a.cin + k * 8 : a.wt, in);
+  }
+  // input row gy into its ring slot (gy + 5) % 5: unit (k, hx)
+  auto load_row = [&](int gy) {
+    const uint32_t slot = ring_a + ((gy + 5) % 5) * SLOT_B;
+    for (int v = tid; v < 130 * KU; v += 128) {
+      const int k = v % KU, hx = v / KU;
+      const int gx = x0 + hx - 1;
+      const bool in = gy >= 0 && gy < a.h && gx >= 0 && gx < a.w;
+      const bf16* src = in ? conv_in(a.x, a.x2, a.cin, a.cs, a.h, a.w, img, gy, gx, k * 8) : a.x;
+      cp_async16(slot + (k * 130 + hx) * 16, src, in);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  load_row(y_begin - 1);
+  load_row(y_begin);
+  load_row(y_begin + 1);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc<N>();
+  bool ok = true;
+  // epilogue of output row y from accumulator (y - y_begin) & 1
+  auto epilogue = [&](int y) {
+    const int b = (y - y_begin) & 1;
+    const bool done = mbar_wait(smem_u32(bar + b), (uint32_t)(((y - y_begin) >> 1) & 1));
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+    if (!ok) return;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const int gx = x0 + warp * 32 + lane;
+    const size_t p = (size_t)(img * a.h + y) * a.w + gx;
+#pragma unroll 1
+    for (int col = 0; col < N; col += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]),
+            "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * N + col)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (gx < a.w) {
+        float f[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          float x = __uint_as_float(v[j]) + bias_s[col + j];
+          if (a.act) x = x > 0.0f ? x : x * kSlope;
+          f[j] = x;
+        }
+        if (a.y_fp32) {
+          float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(a.y) + p * a.cout + col);
+#pragma unroll
+          for (int j = 0; j < 4; j++) o[j] = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+        } else {
+          uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(a.y) + p * a.cout + col);
+          uint32_t w[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+            w[j] = *reinterpret_cast<const uint32_t*>(&b2);
+          }
+          o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+          o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        }
+      }
+    }
+    // the accumulator is read out before its next MMAs are issued
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  };
+  for (int y = y_begin; y < y_end && ok; y++) {
+    // Row y + 2's slot held row y - 3, last read by output row y - 2, whose
+    // MMAs completed before its epilogue (the previous iteration).
+    load_row(y + 2);
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // rows up to y + 1 are in
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t acc_t = tmem + (uint32_t)(((y - y_begin) & 1) * N);
+      const uint64_t db0 = umma_desc(wts_a, LBO_B, 128);
+#pragma unroll
+      for (int tap = 0; tap < 9; tap++) {
+        const int dy = tap / 3, dx = tap - dy * 3;
+        const uint64_t da0 = umma_desc(ring_a + ((y - 1 + dy + 5) % 5) * SLOT_B, LBO_A, 128);
+#pragma unroll
+        for (int st = 0; st < CIN / 16; st++) {
+          const uint64_t da = da0 + (uint64_t)(((2 * st * 130 + dx) * 16) >> 4);
+          const uint64_t db = db0 + (uint64_t)(((tap * KU + 2 * st) * N * 16) >> 4);
+          const uint32_t acc = (tap > 0 || st > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(acc_t),
+              "l"(da), "l"(db), "r"(idesc), "r"(acc));
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar + ((y - y_begin) & 1)))
+                   : "memory");
+    }
+    if (y > y_begin) epilogue(y - 1);
+  }
+  if (ok && y_end > y_begin) epilogue(y_end - 1);
+  if (!ok && tid == 0) atomicExch(err, 1);
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(COLS));
+}
+
 // ------------------------------------------------------- weight gradient --
 // dW[co][tap][ci] += sum over pixels p of dY[p][co] * X[p + tap offset][ci].
 // CTA: 64 output channels (4 warps x 16) x CI (16 or 32) input channels of
@@ -854,8 +1012,46 @@ int launch_tc(const ConvArgs& a, int* err, cudaStream_t s) {
   count_launch();
   return check_launch("conv_tc_kernel");
 }
+// Row-streaming launch: rows per CTA chosen so the grid fills the SMs once
+// at the occupancy the shared memory allows (TMEM: 2 x N columns per CTA).
+template <int N, int CIN>
+int launch_row(const ConvArgs& a, int* err, cudaStream_t s) {
+  constexpr int need = conv_row_smem_bytes<N, CIN>();
+  constexpr int floor_b = 228 * 1024 / (512 / pow2_cols(2 * N) + 1) + 1024;
+  constexpr int smem = need > floor_b ? need : floor_b;
+  static_assert(smem <= 227 * 1024, "shared memory per CTA");
+  static bool ready = false;
+  static int sms = 0;
+  if (!ready) {
+    if (cudaFuncSetAttribute(conv_row_kernel<N, CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return cuda_fail("cudaFuncSetAttribute (conv_row)", cudaGetLastError());
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+    ready = true;
+  }
+  const int per_sm = std::max(1, 228 * 1024 / (smem + 1024));
+  const long segs = (long)((a.w + 127) / 128) * a.n;
+  long rows = ((long)a.h * segs + (long)sms * per_sm - 1) / ((long)sms * per_sm);
+  if (rows < 4) rows = 4;
+  if (rows > a.h) rows = a.h;
+  const dim3 grid((unsigned)(segs * ((a.h + rows - 1) / rows)));
+  conv_row_kernel<N, CIN><<<grid, 128, smem, s>>>(a, (int)rows, err);
+  count_launch();
+  return check_launch("conv_row_kernel");
+}
+
 bool tc_shape(const ConvArgs& a) { return a.cout == 16 || a.cout == 32 || a.cout == 64 || a.cout == 96 || a.cout == 128; }
 int launch_conv_tc(const ConvArgs& a, int* err, cudaStream_t s) {
+  // Layers whose weights and a 5-row ring fit in shared memory at 2 or more
+  // CTAs per SM stream rows (measured 11-19 % faster per layer); 96 -> 32,
+  // at 1 CTA per SM, was 2.3x slower that way and keeps the chunked form,
+  // as do the layers whose weights do not fit.
+  if (a.cout == 32 && a.cin == 16) return launch_row<32, 16>(a, err, s);
+  if (a.cout == 32 && a.cin == 32) return launch_row<32, 32>(a, err, s);
+  if (a.cout == 16 && a.cin == 32) return launch_row<16, 32>(a, err, s);
+  if (a.cout == 64 && a.cin == 32) return launch_row<64, 32>(a, err, s);
+  if (a.cout == 64 && a.cin == 64) return launch_row<64, 64>(a, err, s);
+  if (a.cout == 96 && a.cin == 64) return launch_row<96, 64>(a, err, s);
   switch (a.cout) {
     case 16: return launch_tc<16, 16, 8>(a, err, s);
     case 32: return launch_tc<32, 16, 8>(a, err, s);
