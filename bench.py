@@ -214,6 +214,25 @@ def workload_state(C: np.ndarray, spec: dict) -> np.ndarray:
     return C
 
 
+def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time (every rank calls it; a no-op for one rank)."""
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    return float(t.item())
+
+
+def replica_rate(units_per_rank_step: float, steps: int, ms_max: float, world: int) -> float:
+    """Whole-job rate in millions of units per second: every rank (a replica)
+    processed units_per_rank_step per step, the job took ms_max."""
+    return world * units_per_rank_step * steps / (ms_max / 1e3) / 1e6
+
+
 def time_kernel(torch, fn, reps: int) -> float:
     """Mean ms per call of fn() with CUDA events on the current stream."""
     torch.cuda.synchronize()
@@ -264,15 +283,10 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.synchronize()
     launches = ab.launches() - launches0
     clocks = sampler.stop()
-    ms = start.elapsed_time(end)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(start.elapsed_time(end), world)
     ms_per_step = ms_max / args.steps
     rays_per_step = w * h * spec["spp"]
-    value = world * rays_per_step * args.steps / (ms_max / 1e3) / 1e6
+    value = replica_rate(rays_per_step, args.steps, ms_max, world)
 
     # Per-kernel durations (same stream, CUDA events, after the timed region).
     k0 = args.warmup + args.steps
@@ -520,12 +534,8 @@ def run_batch(args, rank: int, world: int, local_rank: int) -> None:
         end.synchronize()
         launches = ab.launches() - launches0
         clocks = sampler.stop()
-        t = torch.tensor([start.elapsed_time(end)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dist.barrier()
-        ms_max = float(t.item())
-        value = world * total_px * args.steps / (ms_max / 1e3) / 1e6
+        ms_max = max_over_ranks(start.elapsed_time(end), world)
+        value = replica_rate(total_px, args.steps, ms_max, world)
 
         # Per-kernel durations: the graph's kernels launched one by one.
         prof = [b.profile() for _ in range(2)][-1]
@@ -721,12 +731,10 @@ def run_denoise(args, rank: int, world: int, local_rank: int) -> None:
     flops = 2.0 * DENOISER_MACS_PER_PIXEL * W * H
     ms = results["tcgen05"]["ms"]
     achieved = flops / (ms / 1e3) / 1e12
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = max_over_ranks(ms, world)
     line = {
-        "metric": METRIC, "value": round(float(t.item()), 4), "unit": "ms per 1080p frame (denoiser)", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(float(t.item()), 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "metric": METRIC, "value": round(ms_max, 4), "unit": "ms per 1080p frame (denoiser)", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16", "data": "synthetic: rendered forest frame (seed 7, walk frame 0, sun shadows); untrained weights",
         "config": {**spec, "parallelism": f"replicas x{world}",
                    "l2": "per-frame activations (level 0: 96 channels x 2 M pixels x 2 B = 398 MB) exceed the 126 MB L2"},
