@@ -291,12 +291,18 @@ static __device__ __noinline__ float wood_t(const float* P, int id, f3 ro, f3 rd
 struct LeafSolve {
   float x, y, z, dx, dy, dz;  // ray in the leaf frame
   float t, spanx, spany;      // Newton start and the clipped interval
-  float best;                 // petiole tube result
+};
+// The leaf's blade shape (P[b+7], P[b+11], P[b+17], P[b+18]), re-read by
+// the Newton stage from the record rather than carried with the solve.
+struct LeafShape {
   float len, width, curl, twist;
 };
-// Returns true when the leaf box is hit and the Newton solve must run;
-// otherwise the result is s.best.
-__device__ __forceinline__ bool leaf_clip(const float* P, int id, f3 ro, f3 rd, float time, float wind, LeafSolve& s) {
+__device__ __forceinline__ LeafShape leaf_shape(const float* P, int id) {
+  return {__ldg(P + id * 24 + 7), __ldg(P + id * 24 + 11), __ldg(P + id * 24 + 17), __ldg(P + id * 24 + 18)};
+}
+// `tube` is the petiole tube's result.  Returns true when the leaf box is hit
+// and the Newton solve must run; otherwise the result is `tube`.
+__device__ __forceinline__ bool leaf_clip(const float* P, int id, f3 ro, f3 rd, float time, float wind, LeafSolve& s, float& tube) {
   ARBOR_COUNT(kEvLeaf);
   Leaf l = load_leaf(P, id, time, wind);
   f3 q = ro - l.origin;
@@ -306,7 +312,7 @@ __device__ __forceinline__ bool leaf_clip(const float* P, int id, f3 ro, f3 rd, 
   s.dx = dot3(rd, l.u);
   s.dy = dot3(rd, l.v);
   s.dz = dot3(rd, l.n);
-  s.best = tube_t(ro, rd, l.origin, l.origin + l.u * l.stem, 0.0011f, 0.00065f);
+  tube = tube_t(ro, rd, l.origin, l.origin + l.u * l.stem, 0.0011f, 0.00065f);
   f2 span = box_span(mk(s.x, s.y, s.z), mk(s.dx, s.dy, s.dz), mk(-0.001f, -l.width, -0.035f), mk(l.len + 0.001f, l.width, 0.065f));
   if (span.y < fmaxf(0.0001f, span.x)) return false;
   ARBOR_COUNT(kEvNewtonStart);
@@ -314,27 +320,23 @@ __device__ __forceinline__ bool leaf_clip(const float* P, int id, f3 ro, f3 rd, 
   s.t = clampf(t, fmaxf(0.0001f, span.x), span.y);
   s.spanx = span.x;
   s.spany = span.y;
-  s.len = l.len;
-  s.width = l.width;
-  s.curl = l.curl;
-  s.twist = l.twist;
   return true;
 }
-__device__ __forceinline__ float leaf_newton(const LeafSolve& s, float footprint) {
+// The Newton stage; `best` is the petiole tube's result.
+__device__ __forceinline__ float leaf_newton(const LeafSolve& s, const LeafShape& sh, float best, float footprint) {
   const float x = s.x, y = s.y, z = s.z, dx = s.dx, dy = s.dy, dz = s.dz;
   float t = s.t;
-  float best = s.best;
-  float hw2 = s.width * s.width;
+  float hw2 = sh.width * sh.width;
   float bw007 = band_weight(0.007f, footprint);
   for (int k = 0; k < 7; k++) {
     ARBOR_COUNT(kEvNewton);
     float xx = x + dx * t;
     float yy = y + dy * t;
-    float height = leaf_height(xx, yy, s.len, hw2, s.curl, s.twist, bw007);
+    float height = leaf_height(xx, yy, sh.len, hw2, sh.curl, sh.twist, bw007);
     float f = z + dz * t - height;
     const float e = 0.00015f;
-    float hx = (leaf_height(xx + e, yy, s.len, hw2, s.curl, s.twist, bw007) - leaf_height(xx - e, yy, s.len, hw2, s.curl, s.twist, bw007)) / (2.0f * e);
-    float hy = (leaf_height(xx, yy + e, s.len, hw2, s.curl, s.twist, bw007) - leaf_height(xx, yy - e, s.len, hw2, s.curl, s.twist, bw007)) / (2.0f * e);
+    float hx = (leaf_height(xx + e, yy, sh.len, hw2, sh.curl, sh.twist, bw007) - leaf_height(xx - e, yy, sh.len, hw2, sh.curl, sh.twist, bw007)) / (2.0f * e);
+    float hy = (leaf_height(xx, yy + e, sh.len, hw2, sh.curl, sh.twist, bw007) - leaf_height(xx, yy - e, sh.len, hw2, sh.curl, sh.twist, bw007)) / (2.0f * e);
     float deriv = dz - hx * dx - hy * dy;
     if (fabsf(deriv) < 0.00001f) break;
     t -= clampf(f / deriv, -0.13f, 0.13f);
@@ -342,15 +344,16 @@ __device__ __forceinline__ float leaf_newton(const LeafSolve& s, float footprint
   }
   float xx = x + dx * t;
   float yy = y + dy * t;
-  float err = fabsf(z + dz * t - leaf_height(xx, yy, s.len, hw2, s.curl, s.twist, bw007));
-  if (t > 0.0001f && xx > 0.0f && xx < s.len && err < 0.0003f && fabsf(yy) < leaf_width(xx, s.len, s.width, band_weight(0.002f, footprint)))
+  float err = fabsf(z + dz * t - leaf_height(xx, yy, sh.len, hw2, sh.curl, sh.twist, bw007));
+  if (t > 0.0001f && xx > 0.0f && xx < sh.len && err < 0.0003f && fabsf(yy) < leaf_width(xx, sh.len, sh.width, band_weight(0.002f, footprint)))
     best = fminf(best, t);
   return best;
 }
 static __device__ __noinline__ float leaf_t(const float* P, int id, f3 ro, f3 rd, float footprint, float time, float wind) {
   LeafSolve s;
-  if (!leaf_clip(P, id, ro, rd, time, wind, s)) return s.best;
-  return leaf_newton(s, footprint);
+  float tube;
+  if (!leaf_clip(P, id, ro, rd, time, wind, s, tube)) return tube;
+  return leaf_newton(s, leaf_shape(P, id), tube, footprint);
 }
 // Arbor.cu:219
 __device__ __forceinline__ float object_t(const float* P, int id, f3 ro, f3 rd, float footprint, float time, float wind, bool refine) {

@@ -176,23 +176,37 @@ __device__ __forceinline__ void dda_step(const TraceCtx& c, Ray& r) {
   dda_advance(r);
 }
 
-// Pop deferred siblings, deepest first, until one is still accepted
-// (the reference's stack pop and re-test, Arbor.cu:223, 227).
-__device__ __forceinline__ bool pop_next(const TraceCtx& c, Ray& r) {
+// Entry distances of the deferred siblings of one lane, one per BVH level
+// 1-15 (a sibling is deferred below the root only), in shared memory with a
+// stride of 32 floats (the warp's lanes side by side).
+struct SiblingSpans {
+  float* lane;  // &spans[0][lane] of a [15][32] array
+  __device__ __forceinline__ float& at(int level) const { return lane[(level - 1) * 32]; }
+};
+
+// Pop deferred siblings, deepest first, until one is still accepted (the
+// reference's stack pop and re-test, Arbor.cu:223, 227).  A sibling is
+// deferred only when its box test passed, and of that test only the
+// comparison span.x < best depends on the ray's state, so the re-test is
+// that comparison on the span.x recorded at the push: the same decision as
+// reloading the node and repeating the slab test, without the load.
+__device__ __forceinline__ bool pop_next(Ray& r, const SiblingSpans& sib) {
   while (r.pending != 0u) {
     int level = 31 - __clz(r.pending);
     r.pending &= ~(1u << level);
     r.node = (r.node >> (r.depth - level)) ^ 1;
     r.depth = level;
-    float4 lo, hi;
-    load_node(c, r.node, lo, hi);
-    if (node_accept(lo, hi, r.lro, r.linv, r.lbest, r.spanx)) return true;
+    const float sx = sib.at(level);
+    if (sx < r.lbest) {
+      r.spanx = sx;
+      return true;
+    }
   }
   return false;
 }
 
 // One interior step (Arbor.cu:224-225, 227).
-__device__ __forceinline__ void tree_step(const TraceCtx& c, Ray& r) {
+__device__ __forceinline__ void tree_step(const TraceCtx& c, Ray& r, const SiblingSpans& sib) {
   if (r.node >= kCapacity) {
     r.phase = kPhLeaf;
     return;
@@ -209,6 +223,7 @@ __device__ __forceinline__ void tree_step(const TraceCtx& c, Ray& r) {
     if (lh && rh) {
       bool l = lx < rx;
       r.pending |= 1u << r.depth;
+      sib.at(r.depth) = l ? rx : lx;
       r.node = l ? left : left + 1;
       r.spanx = l ? lx : rx;
     } else if (lh) {
@@ -221,7 +236,7 @@ __device__ __forceinline__ void tree_step(const TraceCtx& c, Ray& r) {
     if (r.node >= kCapacity) r.phase = kPhLeaf;
     return;
   }
-  if (pop_next(c, r)) {
+  if (pop_next(r, sib)) {
     r.phase = r.node >= kCapacity ? kPhLeaf : kPhTree;
     return;
   }

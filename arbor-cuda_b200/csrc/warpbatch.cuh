@@ -28,6 +28,7 @@ namespace arbor {
 
 constexpr int kQueue = 8;        // default candidates a lane may queue
 constexpr int kNewtonCap = 64;   // pending Newton solves per warp
+enum JobClass : int { kJobLeaf = 0, kJobWood = 1, kJobMisc = 2, kJobNone = 3 };
 
 // Per-warp shared-memory batch for a queue depth of Q candidates per lane.
 template <int Q>
@@ -37,14 +38,13 @@ struct WarpBatchQ {
   float4 rayO[32];             // owner lane's local ray origin and wind time
   float4 rayD[32];             // owner lane's local ray direction
   LeafSolve solve[kNewtonCap];
-  int prim[kWarpJobs];         // lane-major queue: lane * Q + k
+  int prim[kWarpJobs];         // lane-major queue: lane * Q + k (leaf slot, then record id)
   float fp[kWarpJobs];
-  int type[kWarpJobs];
   float res[kWarpJobs];
-  short leafJob[kWarpJobs];    // compacted job lists (queue indices)
-  short woodJob[kWarpJobs];
-  short miscJob[kWarpJobs];
+  signed char cls[kWarpJobs];  // test class of a queued candidate (JobClass)
+  short job[kWarpJobs];        // compacted job list: leaf clips, wood tests, the rest
   short solveJob[kNewtonCap];
+  float sib[15][32];           // deferred siblings' span.x, BVH levels 1-15 (SiblingSpans)
 };
 using WarpBatch = WarpBatchQ<kQueue>;
 
@@ -52,13 +52,14 @@ using WarpBatch = WarpBatchQ<kQueue>;
 // pending, or its ray is done.
 template <class WB>
 __device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WB& b, int lane, int& nq) {
+  const SiblingSpans sib{&b.sib[0][lane]};
   while (r.phase == kPhDDA || r.phase == kPhTree || r.phase == kPhLeaf || r.phase == kPhTreeEnd) {
     if (r.phase == kPhDDA) {
       dda_step(c, r);
       continue;
     }
     if (r.phase == kPhTree) {
-      tree_step(c, r);
+      tree_step(c, r, sib);
       continue;
     }
     if (r.phase == kPhTreeEnd) {
@@ -66,25 +67,20 @@ __device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WB& b, 
       finish_tree(c, r);
       continue;
     }
-    // an accepted leaf: queue its primitive
-    uint32_t uid = __ldg(c.Order + (r.node - kCapacity));
-    if (uid < (uint32_t)kCapacity) {  // an Order entry past the records is skipped, not read
-      int q = lane * WB::kQ + nq++;
-      b.prim[q] = (int)uid;
-      b.fp[q] = fmaxf(0.000005f, r.lcone * fmaxf(0.05f, r.spanx));
-      b.type[q] = (int)ldg4(c.P, (int)uid * 6).w;
-      if (nq == WB::kQ) {
-        r.phase = kPhBlocked;  // resume with the pop once results are in
-        return;
-      }
-    }
-    if (pop_next(c, r)) {
-      r.phase = r.node >= kCapacity ? kPhLeaf : kPhTree;
-    } else if (nq > 0) {
-      r.phase = kPhTreeEnd;
+    // an accepted leaf: queue its slot (the Order entry and the record are
+    // read when the warp runs its tests, off the traversal's load chain)
+    int q = lane * WB::kQ + nq++;
+    b.prim[q] = r.node - kCapacity;
+    b.fp[q] = fmaxf(0.000005f, r.lcone * fmaxf(0.05f, r.spanx));
+    if (nq == WB::kQ) {
+      r.phase = kPhBlocked;  // resume with the pop once results are in
       return;
+    }
+    if (pop_next(r, sib)) {
+      r.phase = r.node >= kCapacity ? kPhLeaf : kPhTree;
     } else {
-      finish_tree(c, r);
+      r.phase = kPhTreeEnd;  // the tree's queued tests must come back first
+      return;
     }
   }
 }
@@ -98,16 +94,26 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
     b.rayO[lane] = make_float4(r.lro.x, r.lro.y, r.lro.z, r.ltime);
     b.rayD[lane] = make_float4(r.lrd.x, r.lrd.y, r.lrd.z, 0.0f);
   }
-  // per-lane counts by class, scanned across the warp
+  // Resolve each queued leaf slot to its record and test class: leaf clip,
+  // wood (tube + SDF march, primary rays), the rest (stones, shadow-ray wood,
+  // unused records) or none (an Order entry past the records, skipped and
+  // not read).  Per-lane counts by class, scanned across the warp.
   int nl = 0, nw = 0, nm = 0;
   for (int k = 0; k < nq; k++) {
-    int t = b.type[lane * WB::kQ + k];
-    if (t == 1)
-      nl++;
-    else if (t == 0 && c.refine)
-      nw++;
-    else
-      nm++;
+    const int q = lane * WB::kQ + k;
+    const uint32_t uid = __ldg(c.Order + b.prim[q]);
+    int cls = kJobNone;
+    if (uid < (uint32_t)kCapacity) {
+      const int t = (int)ldg4(c.P, (int)uid * 6).w;
+      cls = t == 1 ? kJobLeaf : (t == 0 && c.refine) ? kJobWood : kJobMisc;
+    } else {
+      b.res[q] = kFar;
+    }
+    b.prim[q] = (int)uid;
+    b.cls[q] = (signed char)cls;
+    nl += cls == kJobLeaf;
+    nw += cls == kJobWood;
+    nm += cls == kJobMisc;
   }
   int sl = nl, sw = nw, sm = nm;
 #pragma unroll
@@ -120,16 +126,16 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
     }
   }
   const int totL = __shfl_sync(full, sl, 31), totW = __shfl_sync(full, sw, 31), totM = __shfl_sync(full, sm, 31);
-  int ol = sl - nl, ow = sw - nw, om = sm - nm;
+  int ol = sl - nl, ow = totL + sw - nw, om = totL + totW + sm - nm;
   for (int k = 0; k < nq; k++) {
     int q = lane * WB::kQ + k;
-    int t = b.type[q];
-    if (t == 1)
-      b.leafJob[ol++] = (short)q;
-    else if (t == 0 && c.refine)
-      b.woodJob[ow++] = (short)q;
-    else
-      b.miscJob[om++] = (short)q;
+    int cls = b.cls[q];
+    if (cls == kJobLeaf)
+      b.job[ol++] = (short)q;
+    else if (cls == kJobWood)
+      b.job[ow++] = (short)q;
+    else if (cls == kJobMisc)
+      b.job[om++] = (short)q;
   }
   __syncwarp();
   // Leaf clips, 32 jobs at a time while fewer than 32 Newton solves are
@@ -144,11 +150,12 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
       LeafSolve ls;
       int q = 0;
       if (j < totL) {
-        q = b.leafJob[j];
+        q = b.job[j];
         int owner = q / WB::kQ;
         float4 o = b.rayO[owner], d = b.rayD[owner];
-        solve = leaf_clip(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls);
-        if (!solve) b.res[q] = ls.best;
+        float tube;
+        solve = leaf_clip(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls, tube);
+        b.res[q] = tube;  // the result, or the Newton stage's starting best
       }
       unsigned m = __ballot_sync(full, solve);
       if (solve) {
@@ -165,7 +172,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
     const int run = nN < 32 ? nN : 32;
     if (lane < run) {
       int qn = b.solveJob[lane];
-      b.res[qn] = leaf_newton(b.solve[lane], b.fp[qn]);
+      b.res[qn] = leaf_newton(b.solve[lane], leaf_shape(c.P, b.prim[qn]), b.res[qn], b.fp[qn]);
     }
     __syncwarp();
     if (lane < nN - run) {
@@ -179,7 +186,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
   for (int base = 0; base < totW; base += 32) {
     int j = base + lane;
     if (j < totW) {
-      int q = b.woodJob[j];
+      int q = b.job[totL + j];
       int owner = q / WB::kQ;
       float4 o = b.rayO[owner], d = b.rayD[owner];
       b.res[q] = wood_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], true);
@@ -189,7 +196,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
   for (int base = 0; base < totM; base += 32) {
     int j = base + lane;
     if (j < totM) {
-      int q = b.miscJob[j];
+      int q = b.job[totL + totW + j];
       int owner = q / WB::kQ;
       float4 o = b.rayO[owner], d = b.rayD[owner];
       b.res[q] = object_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], o.w, c.wind, c.refine);
@@ -200,7 +207,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
 
 // Apply a lane's results in candidate order and resume it.
 template <class WB>
-__device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, const WB& b, int lane, int& nq) {
+__device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, WB& b, int lane, int& nq) {
   for (int k = 0; k < nq; k++) {
     float t = b.res[lane * WB::kQ + k];
     if (t < r.lbest) {
@@ -210,7 +217,7 @@ __device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, const WB&
   }
   nq = 0;
   if (r.phase == kPhBlocked) {
-    if (pop_next(c, r))
+    if (pop_next(r, SiblingSpans{&b.sib[0][lane]}))
       r.phase = r.node >= kCapacity ? kPhLeaf : kPhTree;
     else
       finish_tree(c, r);
