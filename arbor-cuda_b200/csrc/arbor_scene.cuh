@@ -391,11 +391,16 @@ __device__ __forceinline__ float object_t(const float* P, int id, f3 ro, f3 rd, 
 // A child reached by descent is not re-tested: the reference's re-test of it
 // repeats the child test just made with the same best, so it always passes;
 // its span.x (the leaf footprint input) is carried instead.
-__device__ __forceinline__ bool node_accept(float4 lo, float4 hi, f3 ro, f3 inv, float best, float& spanx) {
+__device__ __forceinline__ bool node_accept_span(float4 lo, float4 hi, f3 ro, f3 inv, float best, f2& s) {
   ARBOR_COUNT(kEvNode);
-  f2 s = box_span_inv(ro, inv, xyz(lo), xyz(hi));
-  spanx = s.x;
+  s = box_span_inv(ro, inv, xyz(lo), xyz(hi));
   return lo.w > 0.0f && s.y >= fmaxf(0.0001f, s.x) && s.x < best;
+}
+__device__ __forceinline__ bool node_accept(float4 lo, float4 hi, f3 ro, f3 inv, float best, float& spanx) {
+  f2 s;
+  const bool ok = node_accept_span(lo, hi, ro, inv, best, s);
+  spanx = s.x;
+  return ok;
 }
 __device__ __forceinline__ f2 trace_tree(const float* P, const float* Nodes, const uint32_t* Order, f3 ro, f3 rd, float cone, float time,
                                          float wind, float best, int ignore, bool shadows) {

@@ -18,9 +18,11 @@
 // answer, and the answer is the nearest hit over the accepted leaf boxes
 // whatever the order of the tests.  Traversing past a queued candidate with
 // the not-yet-updated best only adds tests that cannot win; the footprint of
-// each test depends only on its own box (Arbor.cu:226).  The one difference is
-// the order in which exactly equal t values are met.  The DDA advance and
-// tree hand-over wait for all results, so they use the reference's best.
+// each test depends only on its own box (Arbor.cu:226).  Between exactly
+// equal t values the reference keeps the one it meets first; batch_apply
+// decides such ties by the reference's visiting order (ref_before).  The DDA
+// advance and tree hand-over wait for all results, so they use the
+// reference's best.
 #pragma once
 #include "tracer.cuh"
 
@@ -42,6 +44,7 @@ struct WarpBatchQ {
   float fp[kWarpJobs];
   float res[kWarpJobs];
   signed char cls[kWarpJobs];  // test class of a queued candidate (JobClass)
+  short slot[kWarpJobs];       // leaf slot of a queued candidate (primary rays)
   short job[kWarpJobs];        // compacted job list: leaf clips, wood tests, the rest
   short solveJob[kNewtonCap];
   float sib[15][32];           // deferred siblings' span.x, BVH levels 1-15 (SiblingSpans)
@@ -71,6 +74,7 @@ __device__ __forceinline__ void batch_advance(const TraceCtx& c, Ray& r, WB& b, 
     // read when the warp runs its tests, off the traversal's load chain)
     int q = lane * WB::kQ + nq++;
     b.prim[q] = r.node - kCapacity;
+    if (c.refine) b.slot[q] = (short)(r.node - kCapacity);
     b.fp[q] = fmaxf(0.000005f, r.lcone * fmaxf(0.05f, r.spanx));
     if (nq == WB::kQ) {
       r.phase = kPhBlocked;  // resume with the pop once results are in
@@ -205,14 +209,25 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
   __syncwarp();
 }
 
-// Apply a lane's results in candidate order and resume it.
+// Apply a lane's results and resume it.  A nearer hit replaces the best.  For
+// primary rays (visited in their own order) an exactly equal one replaces it
+// when the reference meets it first, so the kept primitive does not depend on
+// the order of visits or tests; shadow segments visit in the reference's
+// order, in which the first of equal hits is kept as it is.
 template <class WB>
 __device__ __forceinline__ void batch_apply(const TraceCtx& c, Ray& r, WB& b, int lane, int& nq) {
   for (int k = 0; k < nq; k++) {
-    float t = b.res[lane * WB::kQ + k];
-    if (t < r.lbest) {
+    const int q = lane * WB::kQ + k;
+    const float t = b.res[q];
+    if (c.refine) {
+      const int slot = b.slot[q];
+      if (t < r.lbest || (t == r.lbest && r.lfound >= 0 && ref_before(c, r, slot, r.lfound))) {
+        r.lbest = t;
+        r.lfound = slot;
+      }
+    } else if (t < r.lbest) {
       r.lbest = t;
-      r.lfound = b.prim[lane * WB::kQ + k];
+      r.lfound = b.prim[q];
     }
   }
   nq = 0;
