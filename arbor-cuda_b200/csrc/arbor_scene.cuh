@@ -208,6 +208,26 @@ __device__ __forceinline__ float leaf_height(float u, float v, float len, float 
   float mid = 0.0012f * expf(-fabsf(v) / 0.005f) * s * bw007;
   return coarse + mid;
 }
+// leaf_height in parts, for the Newton stage's five evaluations at
+// (u, v), (u +- e, v), (u, v +- e): the along-blade terms of one u and the
+// across-blade terms of one v are each computed once and shared.  Each
+// height is assembled with exactly leaf_height's operations.
+struct LeafU {
+  float q, s;
+};
+struct LeafV {
+  float vv, ev;  // v * v / hw2, expf(-|v| / 0.005)
+};
+__device__ __forceinline__ LeafU leaf_u(float u, float len) {
+  const float q = clampf(u / len, -0.2f, 1.2f);
+  return {q, sinf(kPi * q)};
+}
+__device__ __forceinline__ LeafV leaf_v(float v, float hw2) { return {v * v / hw2, expf(-fabsf(v) / 0.005f)}; }
+__device__ __forceinline__ float leaf_height_parts(const LeafU& a, float v, const LeafV& b, float curl, float twist, float bw007) {
+  float coarse = curl * a.s + twist * (a.q - 0.4f) * v + 0.009f * b.vv * a.s;
+  float mid = 0.0012f * b.ev * a.s * bw007;
+  return coarse + mid;
+}
 
 // ------------------------------------------------------- intersections --
 // Arbor.cu:186
@@ -332,11 +352,13 @@ __device__ __forceinline__ float leaf_newton(const LeafSolve& s, const LeafShape
     ARBOR_COUNT(kEvNewton);
     float xx = x + dx * t;
     float yy = y + dy * t;
-    float height = leaf_height(xx, yy, sh.len, hw2, sh.curl, sh.twist, bw007);
-    float f = z + dz * t - height;
     const float e = 0.00015f;
-    float hx = (leaf_height(xx + e, yy, sh.len, hw2, sh.curl, sh.twist, bw007) - leaf_height(xx - e, yy, sh.len, hw2, sh.curl, sh.twist, bw007)) / (2.0f * e);
-    float hy = (leaf_height(xx, yy + e, sh.len, hw2, sh.curl, sh.twist, bw007) - leaf_height(xx, yy - e, sh.len, hw2, sh.curl, sh.twist, bw007)) / (2.0f * e);
+    const LeafU u0 = leaf_u(xx, sh.len), up = leaf_u(xx + e, sh.len), um = leaf_u(xx - e, sh.len);
+    const LeafV v0 = leaf_v(yy, hw2), vp = leaf_v(yy + e, hw2), vm = leaf_v(yy - e, hw2);
+    float height = leaf_height_parts(u0, yy, v0, sh.curl, sh.twist, bw007);
+    float f = z + dz * t - height;
+    float hx = (leaf_height_parts(up, yy, v0, sh.curl, sh.twist, bw007) - leaf_height_parts(um, yy, v0, sh.curl, sh.twist, bw007)) / (2.0f * e);
+    float hy = (leaf_height_parts(u0, yy + e, vp, sh.curl, sh.twist, bw007) - leaf_height_parts(u0, yy - e, vm, sh.curl, sh.twist, bw007)) / (2.0f * e);
     float deriv = dz - hx * dx - hy * dy;
     if (fabsf(deriv) < 0.00001f) break;
     t -= clampf(f / deriv, -0.13f, 0.13f);

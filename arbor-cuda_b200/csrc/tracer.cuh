@@ -220,20 +220,23 @@ __device__ __forceinline__ bool pop_next(Ray& r, const SiblingSpans& sib) {
 // every node, the child with the smaller entry span.x goes first (the left
 // one only when its entry is strictly smaller).  The two leaves part at their
 // lowest common ancestor, so the order is that node's decision, made again
-// here on the same values.
-__device__ __forceinline__ bool ref_before(const TraceCtx& c, const Ray& r, int a, int b) {
+// here on the same values (ro, inv: the tree-local ray).  Ties are rare; the
+// function stays out of line, away from the traversal's instruction stream.
+static __device__ __noinline__ bool ref_before_at(const float* __restrict__ Nodes, f3 ro, f3 inv, int a, int b) {
   int na = a + kCapacity, nb = b + kCapacity;
   while ((na >> 1) != (nb >> 1)) {
     na >>= 1;
     nb >>= 1;
   }
   const int left = na & ~1;
-  float4 llo, lhi, rlo, rhi;
-  load_node(c, left, llo, lhi);
-  load_node(c, left + 1, rlo, rhi);
-  const float lx = box_span_inv(r.lro, r.linv, xyz(llo), xyz(lhi)).x;
-  const float rx = box_span_inv(r.lro, r.linv, xyz(rlo), xyz(rhi)).x;
+  const float4 llo = ldg4(Nodes, 2 * left), lhi = ldg4(Nodes, 2 * left + 1);
+  const float4 rlo = ldg4(Nodes, 2 * left + 2), rhi = ldg4(Nodes, 2 * left + 3);
+  const float lx = box_span_inv(ro, inv, xyz(llo), xyz(lhi)).x;
+  const float rx = box_span_inv(ro, inv, xyz(rlo), xyz(rhi)).x;
   return (na == left) == (lx < rx);
+}
+__device__ __forceinline__ bool ref_before(const TraceCtx& c, const Ray& r, int a, int b) {
+  return ref_before_at(c.Nodes, r.lro, r.linv, a, b);
 }
 
 // One interior step (Arbor.cu:224-225, 227).
