@@ -207,6 +207,26 @@ struct Shading {
   bool shadow;  // visibility must be traced
 };
 
+// The pixel's light direction: the sun jittered inside its disk by the
+// pixel's and sample's hashes (Arbor.cu:282).
+__device__ __forceinline__ f3 sun_sample(const Camera& cam, int pixel) {
+  const f3 sun = cam.sun;
+  int sample = cam.sample;
+  float r1 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 1823u), 991);
+  float r2 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 971u), 731);
+  f3 su = basisU(sun);
+  f3 sv = cross3(sun, su);
+  float angle = r1 * 6.28318f;
+  float disk = sqrtf(r2) * 0.012f;
+  return norm3(sun + su * (xcos(angle) * disk) + sv * (xsin(angle) * disk));
+}
+// The first shadow segment's origin, off the surface along the light
+// (Arbor.cu:283).
+__device__ __forceinline__ f3 shadow_origin(f3 p, f3 light, int id) {
+  float offset = id >= 0 ? 0.0014f : 0.004f;
+  return p + light * offset;
+}
+
 // The single-tree scene uses the identity instance: tree-local point and
 // normal, phase 0, no tint.
 template <bool kForestScene>
@@ -292,17 +312,9 @@ __device__ __noinline__ void shade_pre(const float* P, const Camera& cam, const 
     return;
   }
   o.final = false;
-  int sample = cam.sample;
-  float r1 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 1823u), 991);
-  float r2 = rnd((int)((uint32_t)pixel + (uint32_t)sample * 971u), 731);
-  f3 su = basisU(sun);
-  f3 sv = cross3(sun, su);
-  float angle = r1 * 6.28318f;
-  float disk = sqrtf(r2) * 0.012f;
-  f3 light = norm3(sun + su * (xcos(angle) * disk) + sv * (xsin(angle) * disk));
-  float offset = id >= 0 ? 0.0014f : 0.004f;
+  const f3 light = sun_sample(cam, pixel);
   o.light = light;
-  o.origin = p + light * offset;
+  o.origin = shadow_origin(p, light, id);
   o.shadow = cam.shadows > 0.5f;
   float nl = sat(dot3(n, light));
   float back = sat(-dot3(n, light));
@@ -403,6 +415,89 @@ __device__ __forceinline__ void shade_tile(const TraceCtx& c, const Camera& cam,
   r.phase = kPhIdle;
   if (x < width && y < height) policy.start(c, r, x, y);
   batch_run(c, r, b, policy);
+}
+
+// The shadow ray of pixel (x, y), when shadePixels traces one: a surface hit
+// (not sky), no debug view, sun shadows on.  The same values shade_pre
+// computes for the pixel.
+__device__ __forceinline__ bool shadow_ray(const Camera& cam, float4 hit, int x, int y, int width, int height, f3& origin, f3& light) {
+  const float t = hit.x;
+  int id = (int)hit.y;
+  if (id >= kCapacity) id = -1;
+  if (!(t < kFar) || cam.mode == 1.0f || cam.mode == 2.0f || cam.mode == 3.0f || !(cam.shadows > 0.5f)) return false;
+  const f3 p = cam.ro + camera_ray(cam, x, y, width, height) * t;
+  light = sun_sample(cam, y * width + x);
+  origin = shadow_origin(p, light, id);
+  return true;
+}
+
+// Shadow segments alone (Arbor.cu:271-274), for the persistent shadow pass:
+// a pixel's visibility toward the sun is written to Vis (the Linear buffer,
+// which the compose pass then overwrites with the colour); pixels without a
+// shadow ray are left alone.
+struct ShadowPolicy {
+  static constexpr int kRefill = 8;
+  const TraceCtx* ctx;
+  const Camera* cam;
+  const float* Hit;
+  float* Vis;
+  int width, height;
+  int pixel, seg;
+  f3 trans, origin, light;
+  __device__ __forceinline__ void start(const TraceCtx& c, Ray& r, int x, int y) {
+    pixel = y * width + x;
+    if (shadow_ray(*cam, __ldg(reinterpret_cast<const float4*>(Hit) + pixel), x, y, width, height, origin, light)) {
+      trans = mk(1.0f, 1.0f, 1.0f);
+      seg = 0;
+      ray_begin(c, r, origin, light, 36.0f);
+    } else {
+      r.phase = kPhIdle;
+    }
+  }
+  __device__ __forceinline__ void write(f3 v) { reinterpret_cast<float4*>(Vis)[pixel] = make_float4(v.x, v.y, v.z, 1.0f); }
+  __device__ __forceinline__ void done(Ray& r) {
+    int id = (int)r.found;
+    if (id < 0) {
+      write(trans);
+    } else if (ldg4(ctx->P, id * 6).w != 1.0f) {
+      write(mk(0.0f, 0.0f, 0.0f));
+    } else {
+      trans = trans * mk(0.18f, 0.29f, 0.065f);
+      origin = origin + light * (r.best + 0.0018f);
+      if (++seg < 4) {
+        ray_begin(*ctx, r, origin, light, 36.0f);
+        return;
+      }
+      write(trans);
+    }
+    r.phase = kPhIdle;
+  }
+};
+
+// Shadow segments of every pixel of a persistent CTA's pool.
+template <class WB>
+__device__ __forceinline__ void shadow_pool(const TraceCtx& c, const Camera& cam, WB& b, const float* __restrict__ Hit, float* __restrict__ Vis,
+                                            const PixelPool& pool) {
+  ShadowPolicy policy{&c, &cam, Hit, Vis, pool.width, pool.height, 0, 0};
+  Ray r;
+  batch_run_pool(c, r, b, policy, pool);
+}
+
+// shadePixels' colour of pixel (x, y) (Arbor.cu:277-289), its visibility
+// read from Linear where the shadow pass traced one.
+template <bool kForestScene>
+__device__ __forceinline__ void shade_compose_px(const float* __restrict__ P, const Camera& cam, const Instance* inst, const float* __restrict__ Hit,
+                                                 float* __restrict__ Linear, float* __restrict__ Guide, float* __restrict__ Normal, int x, int y,
+                                                 int width, int height) {
+  const int pixel = y * width + x;
+  Shading sh;
+  shade_pre<kForestScene>(P, cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + pixel), x, y, width, height, sh);
+  f3 vis = mk(1.0f, 1.0f, 1.0f);
+  if (!sh.final && sh.shadow) vis = xyz(reinterpret_cast<const float4*>(Linear)[pixel]);
+  const f3 col = shade_post(sh, vis);
+  reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
+  reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);
+  if (Normal) reinterpret_cast<float4*>(Normal)[pixel] = make_float4(sh.normal.x, sh.normal.y, sh.normal.z, 0.0f);
 }
 
 // ------------------------------------------------------ filter / resolve --

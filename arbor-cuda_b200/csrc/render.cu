@@ -2,12 +2,12 @@
 // filterLighting, resolvePixels (Arbor.cu:252-304) and their single-tree and
 // fused variants, with their C-ABI entry points.
 //
-// Launch shapes: the trace is persistent (2 CTAs per SM, lanes taking pixels
-// of 8x4 blocks as their rays finish); the shade runs 256-thread blocks over
-// 16x16 pixel tiles, each warp an 8x4 sub-tile so neighbouring rays share
-// traversal paths.  Each trace/shade block builds the 324-entry forest
-// instance table in shared memory once; every table entry equals what the
-// reference's forest helpers recompute per ray (Arbor.cu:57-69).
+// Launch shapes: the trace and the shade's shadow pass are persistent (2
+// CTAs per SM, lanes taking pixels of 8x4 blocks as their rays finish); the
+// shade's compose pass runs 256-thread blocks over 16x16 pixel tiles.  Each
+// block builds the 324-entry forest instance table in shared memory once;
+// every table entry equals what the reference's forest helpers recompute per
+// ray (Arbor.cu:57-69).
 #include <algorithm>
 
 #include "abi_util.h"
@@ -17,22 +17,6 @@ namespace arbor {
 namespace {
 
 // ---------------------------------------------------------------- kernels --
-// Shading: one pixel per thread over 16x16-pixel CTAs (8x4-pixel warps);
-// each warp's shadow-ray primitive tests run warp-batched (warpbatch.cuh).
-template <bool kForestScene>
-__global__ void __launch_bounds__(kBlock, 2) shade_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
-                                                          const uint32_t* __restrict__ Order, const float* __restrict__ C,
-                                                          const float* __restrict__ Hit, float* __restrict__ Linear,
-                                                          float* __restrict__ Guide, float* __restrict__ Normal, int width, int height) {
-  extern __shared__ float4 batch_smem[];
-  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
-  __shared__ Camera cam;
-  __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
-  const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
-  shade_tile<kForestScene>(c, cam, inst, b, P, Hit, Linear, Guide, width, height, blockIdx.x * kTile, blockIdx.y * kTile, kTile, Normal);
-}
-
 // Persistent form of the trace: a grid of (SMs x 2) CTAs, each taking every
 // gridDim.x-th 8x4-pixel block of the image, its lanes taking pixels as
 // their rays finish (batch_run_pool).
@@ -51,6 +35,41 @@ __global__ void __launch_bounds__(kBlock, 2) trace_pool_kernel(const float* __re
   const int bx = (width + 7) / 8;
   const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
   trace_pool(c, cam, b, Hit, pool);
+}
+
+// shadePixels in two passes.  The shadow pass is persistent like the trace:
+// lanes take pixels from a pool and trace their shadow segments, writing the
+// visibility into Linear; with sun shadows off it returns at once.
+template <bool kForestScene>
+__global__ void __launch_bounds__(kBlock, 2) shadow_pool_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                                const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                                const float* __restrict__ Hit, float* __restrict__ Linear, int width, int height) {
+  extern __shared__ float4 batch_smem[];
+  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForestScene ? kForest : 1];
+  __shared__ int next;
+  if (threadIdx.x == 0) next = 0;
+  block_setup(C, cam, inst, kForestScene);
+  if (!(cam.shadows > 0.5f)) return;
+  const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
+  const int bx = (width + 7) / 8;
+  const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
+  shadow_pool(c, cam, b, Hit, Linear, pool);
+}
+
+// The compose pass: one pixel per thread, the surface terms and the colour
+// with the shadow pass's visibility.
+template <bool kForestScene>
+__global__ void __launch_bounds__(kBlock) shade_compose_kernel(const float* __restrict__ P, const float* __restrict__ C, const float* __restrict__ Hit,
+                                                               float* __restrict__ Linear, float* __restrict__ Guide, float* __restrict__ Normal,
+                                                               int width, int height) {
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForestScene ? kForest : 1];
+  block_setup(C, cam, inst, kForestScene);
+  int x, y;
+  tile_pixel_at(threadIdx.x, blockIdx.x * kTile, blockIdx.y * kTile, kTile, x, y);
+  if (x < width && y < height) shade_compose_px<kForestScene>(P, cam, inst, Hit, Linear, Guide, Normal, x, y, width, height);
 }
 
 template <bool kResolve>
@@ -144,18 +163,20 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
     if (int s = check_bindings(name, g)) return s;
   }
   if (empty) return ARBOR_OK;
-  if (!batch_smem_ready(forest ? (const void*)shade_kernel<true> : (const void*)shade_kernel<false>)) {
+  if (!batch_smem_ready(forest ? (const void*)shadow_pool_kernel<true> : (const void*)shadow_pool_kernel<false>)) {
     set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
     return ARBOR_ERR_CUDA;
   }
-  // Shading stays on fixed tiles: its per-pixel start (surface terms,
-  // normals) is long, and refilling lanes one by one ran it with few lanes
-  // active (measured slower than tiles).
-  if (forest)
-    shade_kernel<true><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, Normal, width, height);
-  else
-    shade_kernel<false><<<pixel_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, Normal, width, height);
-  count_launch();
+  // Shadow segments in a persistent pass whose loop holds only the tracer
+  // (its code stays small), then the shading of every pixel.
+  if (forest) {
+    shadow_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, width, height);
+    shade_compose_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, Normal, width, height);
+  } else {
+    shadow_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, width, height);
+    shade_compose_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, Normal, width, height);
+  }
+  count_launch(2);
   return check_launch(name);
 }
 
