@@ -337,9 +337,13 @@ __device__ __forceinline__ f3 shade_post(const Shading& o, f3 visibility) {
   return mix3(col, o.skyc, o.haze);
 }
 
-// Shadow segments (Arbor.cu:271-274: at most four forest traces toward the
-// sun, 36 m, leaf transmission, any other hit opaque) run through the same
-// warp-batched tracer; a pixel without a shadow ray finishes when shaded.
+// shadePixels in one pass, for the batched renderer's tiles: the surface
+// terms, then the shadow segments (Arbor.cu:271-274: at most four forest
+// traces toward the sun, 36 m, leaf transmission, any other hit opaque)
+// through the same warp-batched tracer; a pixel without a shadow ray
+// finishes when shaded.  (The single-image shadePixels runs the shadow
+// segments and the shading as separate passes; in the batch's tile kernel
+// that split measured slower than this fused form.)
 template <bool kForestScene>
 struct ShadePolicy {
   const float* P;
