@@ -73,15 +73,29 @@ def flops(counts: dict) -> int:
     return int(sum(WEIGHTS[k] * counts[k] for k in EVENTS))
 
 
-def roofline_entry(kernel: str, counts: dict, pixels: int, ms: float, fp32_peak_tops: float, sm_clock_mhz: float) -> dict:
+# DRAM traffic per unit, measured with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) on one 960x544 launch of the forest walk's first
+# frame (seed 7, cold caches): the trace kernel moved 5.33 MB for 522,240
+# primary rays, the shadow pass of shadePixels 13.85 MB for 522,240 pixels.
+# The 5.7 MB scene stays in L2, so the traffic grows with the pixel count;
+# bench lines scale these to their launch.
+TRACE_DRAM_BYTES_PER_RAY = 10.2
+SHADOW_DRAM_BYTES_PER_PIXEL = 26.5
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 960x544 forest launch, scaled by units to this launch"
+
+
+def roofline_entry(kernel: str, counts: dict, pixels: int, ms: float, fp32_peak_tops: float, sm_clock_mhz: float,
+                   traffic: int | None = None, traffic_source: str | None = None) -> dict:
     """FP32 roofline line of one launch whose counted events are `counts`
-    over `pixels` pixels, timed at `ms` per launch."""
+    over `pixels` pixels, timed at `ms` per launch; `traffic` is the
+    launch's DRAM bytes where a capture of the kernel exists."""
     ops = flops(counts)
     achieved = ops / (ms / 1e3) / 1e12
     pixels = max(1, pixels)
     return {
         "kernel": kernel, "bound": "fp32", "achieved": round(achieved, 3), "peak": round(fp32_peak_tops, 2),
-        "unit": "TFLOP/s", "frac": round(achieved / fp32_peak_tops, 4), "traffic": None,
+        "unit": "TFLOP/s", "frac": round(achieved / fp32_peak_tops, 4), "traffic": traffic,
+        **({"traffic_source": traffic_source} if traffic is not None else {}),
         "algorithmic_flops": ops, "flops_per_pixel": round(ops / pixels, 1),
         "events_per_pixel": {k: round(v / pixels, 3) for k, v in counts.items() if v},
         "peak_source": f"derived: 148 SM x 128 FP32 lanes x {sm_clock_mhz:.0f} MHz measured SM clock, one non-fused op per lane per "
@@ -92,9 +106,14 @@ def roofline_entry(kernel: str, counts: dict, pixels: int, ms: float, fp32_peak_
 
 def trace_roofline(ab, fr, torch, ms_trace: float, fp32_peak_tops: float, sm_clock_mhz: float) -> dict:
     counts = count_events(ab, fr.P, fr.Nodes, fr.Order, fr.C, fr.w, fr.h, fr.spec["single_tree"], torch)
-    return roofline_entry("tracePixels", counts, fr.w * fr.h, ms_trace, fp32_peak_tops, sm_clock_mhz)
+    traffic = None if fr.spec["single_tree"] else int(TRACE_DRAM_BYTES_PER_RAY * fr.w * fr.h)
+    return roofline_entry("tracePixels", counts, fr.w * fr.h, ms_trace, fp32_peak_tops, sm_clock_mhz, traffic,
+                          TRAFFIC_SOURCE + " (trace_pool_kernel)")
 
 
 def shade_roofline(ab, fr, torch, ms_shade: float, fp32_peak_tops: float, sm_clock_mhz: float) -> dict:
     counts = count_events(ab, fr.P, fr.Nodes, fr.Order, fr.C, fr.w, fr.h, fr.spec["single_tree"], torch, Hit=fr.Hit)
-    return roofline_entry("shadePixels", counts, fr.w * fr.h, ms_shade, fp32_peak_tops, sm_clock_mhz)
+    shadows = bool(fr.spec.get("shadows")) and not fr.spec["single_tree"]
+    traffic = int(SHADOW_DRAM_BYTES_PER_PIXEL * fr.w * fr.h) if shadows else None
+    return roofline_entry("shadePixels", counts, fr.w * fr.h, ms_shade, fp32_peak_tops, sm_clock_mhz, traffic,
+                          TRAFFIC_SOURCE + " (shadow_pool_kernel; the compose pass, 64 B/px, is not included)")
