@@ -239,7 +239,8 @@ def main() -> None:
     check(lib.arbor_denoiser_destroy(hd))
     mean = {k: round(float(np.mean(v)), 3) for k, v in scores.items()}
     result = {
-        "denoiser": "4-level U-Net 32/64/96/128, 3x3, BF16 weights and activations, FP32 accumulation (mma.sync m16n8k16)",
+        "denoiser": "4-level U-Net 32/64/96/128, 3x3, BF16 weights and activations, FP32 accumulation; forward "
+                    "convolutions on tcgen05 (TMEM accumulators), backward on mma.sync m16n8k16",
         "data": {"train_views": args.train_views, "eval_views": args.eval_views, "size": S, "spp_target": args.spp, "scenes": args.scenes,
                  "render_seconds": round(t_data, 1)},
         "train": {"steps": args.steps, "batch": args.batch, "lr": args.lr, "seconds": round(t_train, 2),
