@@ -1,16 +1,20 @@
 // batch.cu - batched multi-view rendering.
 //
 // Many views (each with its own resolution, camera record C and resident
-// scene) render in one CUDA graph launch of four kernels:
+// scene) render in one CUDA graph launch of five kernels:
 //
 //   batch_setup_kernel        per view: camera constants, the forest
 //                             instance table and the filter/resolve scalars
-//                             of its C record; resets the tile queues
-//   batch_pass_kernel<trace>  persistent CTAs pull tiles of every view from
+//                             of its C record; resets the queues
+//   batch_pass_kernel         persistent CTAs pull tiles of every view from
 //                             one global queue and run tracePixels
 //                             (Arbor.cu:252) on each
-//   batch_pass_kernel<shade>  the same over the same tiles for shadePixels
-//                             (Arbor.cu:277-289)
+//   batch_shadow_kernel       persistent warps walk the views; in each, their
+//                             lanes take pixels from the view's own queue
+//                             as their rays finish and trace the shadow
+//                             segments of shadePixels (Arbor.cu:271-274)
+//   batch_compose_kernel      the trace tiles again: shadePixels' colours
+//                             (Arbor.cu:277-289) with that visibility
 //   batch_filter_kernel       persistent CTAs pull 32x8 tiles and run the
 //                             fused filterLighting + resolvePixels
 //                             (Arbor.cu:292-304)
@@ -21,10 +25,10 @@
 // the same C, apart from the order in which exactly equal hit distances are
 // met (the warp batch groups rays by tile; see warpbatch.cuh).
 //
-// The autotuner times the trace and shade kernels on a sample of the views
-// for each tile shape (16x16 or 32x8), CTAs per SM (1 or 2), tile order (view
-// by view, or the largest views first) and warp-batch queue depth (4 or 8
-// candidates per lane), and keeps the fastest.
+// The autotuner times the trace, shadow and compose kernels on a sample of
+// the views for each tile shape (16x16 or 32x8), CTAs per SM (1 or 2), tile
+// order (view by view, or the largest views first) and warp-batch queue
+// depth (4 or 8 candidates per lane), and keeps the fastest.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -36,6 +40,10 @@
 
 namespace arbor {
 namespace {
+
+// Work queues (global counters) of one render: the trace tiles, the compose
+// tiles, the filter tiles, then one pixel queue per view for the shadow pass.
+constexpr int kQueueTrace = 0, kQueueCompose = 1, kQueueFilter = 2, kViewQueues = 3;
 
 struct BatchView {
   const float* P;
@@ -53,6 +61,7 @@ struct BatchView {
 __global__ void __launch_bounds__(kBlock) batch_setup_kernel(const float* __restrict__ Cs, Camera* __restrict__ cams, float4* __restrict__ scal,
                                                              Instance* __restrict__ insts, int* __restrict__ counters) {
   const int v = blockIdx.x;
+  if (threadIdx.x == 0) counters[kViewQueues + v] = 0;
   const float* C = Cs + v * 64;
   if (threadIdx.x == 0) {
     Camera cam;
@@ -62,13 +71,12 @@ __global__ void __launch_bounds__(kBlock) batch_setup_kernel(const float* __rest
   }
   const int ws = (int)C[31];
   for (int t = threadIdx.x; t < kForest; t += blockDim.x) insts[v * kForest + t] = make_instance(t, ws);
-  if (v == 0 && threadIdx.x < 3) counters[threadIdx.x] = 0;
+  if (v == 0 && threadIdx.x < kViewQueues) counters[threadIdx.x] = 0;
 }
 
-// kShade false: tracePixels of each tile; true: shadePixels of each tile
-// (reading the Hit records the trace pass wrote).  Two kernels rather than
-// one fused pass keep each pass's register allocation free of the other's.
-template <int Q, bool kShade>
+// tracePixels of each tile.  The shade runs as separate kernels: their
+// register allocation and code stay out of the trace's loop.
+template <int Q>
 __global__ void __launch_bounds__(kBlock, 2) batch_pass_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
                                                                const Instance* __restrict__ insts, const int4* __restrict__ tiles,
                                                                int n_tiles, int tw, int* __restrict__ counter) {
@@ -92,13 +100,63 @@ __global__ void __launch_bounds__(kBlock, 2) batch_pass_kernel(const BatchView* 
       __syncthreads();
     }
     const BatchView v = views[cur];
-    if (!kShade) {
-      const TraceCtx c{v.P, v.Nodes, v.Order, inst, cam.c14 / (float)v.height, cam.time, cam.wind, true, true};
-      trace_tile(c, cam, b, v.Hit, v.width, v.height, td.y, td.z, tw);
-    } else {
-      const TraceCtx c{v.P, v.Nodes, v.Order, inst, 0.0001f, cam.time, cam.wind, false, true};
-      shade_tile<true>(c, cam, inst, b, v.P, v.Hit, v.Linear, v.Guide, v.width, v.height, td.y, td.z, tw);
+    const TraceCtx c{v.P, v.Nodes, v.Order, inst, cam.c14 / (float)v.height, cam.time, cam.wind, true, true};
+    trace_tile(c, cam, b, v.Hit, v.width, v.height, td.y, td.z, tw);
+    __syncthreads();  // every thread has read s_tile, cam and inst
+  }
+}
+
+// The shadow segments of every view (visibility into its Linear image).
+// Each warp walks the views in order and joins each one's pixel queue; its
+// lanes take the view's next pixels as their rays finish, so warps of any
+// CTA share a view's work and move on independently.  The view's camera and
+// instance table are read from global memory (the same values setup wrote).
+template <int Q>
+__global__ void __launch_bounds__(kBlock, 2) batch_shadow_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
+                                                                 const Instance* __restrict__ insts, const int* __restrict__ list, int n_list,
+                                                                 int* __restrict__ queues) {
+  using WB = WarpBatchQ<Q>;
+  extern __shared__ float4 batch_smem[];
+  WB& b = reinterpret_cast<WB*>(batch_smem)[threadIdx.x >> 5];
+  for (int i = 0; i < n_list; i++) {
+    const int v = __ldg(list + i);
+    const Camera& cam = cams[v];
+    if (!(cam.shadows > 0.5f)) continue;
+    const BatchView view = views[v];
+    const TraceCtx c{view.P, view.Nodes, view.Order, insts + (size_t)v * kForest, 0.0001f, cam.time, cam.wind, false, true};
+    const int bx = (view.width + 7) / 8;
+    const ViewPool pool{queues + v, view.width, view.height, bx, bx * ((view.height + 3) / 4)};
+    ShadowPolicy policy{&c, &cam, view.Hit, view.Linear, view.width, view.height, 0, 0};
+    Ray r;
+    batch_run_pool(c, r, b, policy, pool);
+  }
+}
+
+// shadePixels' colours of each trace tile, one pixel per thread, with the
+// shadow pass's visibility.
+__global__ void __launch_bounds__(kBlock) batch_compose_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
+                                                               const Instance* __restrict__ insts, const int4* __restrict__ tiles,
+                                                               int n_tiles, int tw, int* __restrict__ counter) {
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForest];
+  __shared__ int s_tile;
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= n_tiles) break;
+    const int4 td = __ldg(tiles + t);
+    if (td.x != cur) {  // uniform across the CTA
+      cur = td.x;
+      if (threadIdx.x == 0) cam = cams[cur];
+      for (int k = threadIdx.x; k < kForest; k += blockDim.x) inst[k] = insts[cur * kForest + k];
+      __syncthreads();
     }
+    const BatchView v = views[cur];
+    int x, y;
+    tile_pixel_at(threadIdx.x, td.y, td.z, tw, x, y);
+    if (x < v.width && y < v.height) shade_compose_px<true>(v.P, cam, inst, v.Hit, v.Linear, v.Guide, nullptr, x, y, v.width, v.height);
     __syncthreads();  // every thread has read s_tile, cam and inst
   }
 }
@@ -169,7 +227,8 @@ struct arbor_batch {
   Camera* cams = nullptr;
   float4* scal = nullptr;
   Instance* insts = nullptr;
-  int* counters = nullptr;     // trace, shade and filter tile queues
+  int* counters = nullptr;     // work queues: kViewQueues tile queues, then one pixel queue per view
+  int* vlist = nullptr;        // views the shadow pass walks, in order
   int4* tiles = nullptr;       // trace/shade tiles, then filter tiles
   int n_ts = 0, n_filter = 0;
   size_t tile_capacity = 0;
@@ -210,26 +269,45 @@ int launch_setup(arbor_batch* b, cudaStream_t s) {
   return check_launch("batch_setup_kernel");
 }
 
-// The trace pass then the shade pass over the same tile list.
-int launch_trace_shade(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, cudaStream_t s) {
+// The trace pass over the tile list.
+int launch_trace(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, cudaStream_t s) {
   const dim3 grid(b->sms * cfg.ctas_per_sm);
-  int* ctr = b->counters;
-  if (cfg.queue == 4) {
-    batch_pass_kernel<4, false><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr);
-    batch_pass_kernel<4, true><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr + 1);
-  } else {
-    batch_pass_kernel<8, false><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr);
-    batch_pass_kernel<8, true><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr + 1);
-  }
+  int* ctr = b->counters + kQueueTrace;
+  if (cfg.queue == 4)
+    batch_pass_kernel<4><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr);
+  else
+    batch_pass_kernel<8><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr);
   return check_launch("batch_pass_kernel");
 }
 
-// Rebuild the tile lists for cfg and capture setup -> trace -> shade -> filter.
+// shadePixels: the shadow pass over the listed views, then the compose pass
+// over the tile list.
+int launch_shade(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, int n_list, cudaStream_t s) {
+  const dim3 grid(b->sms * cfg.ctas_per_sm);
+  int* queues = b->counters + kViewQueues;
+  if (cfg.queue == 4)
+    batch_shadow_kernel<4><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
+  else
+    batch_shadow_kernel<8><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
+  if (int st = check_launch("batch_shadow_kernel")) return st;
+  batch_compose_kernel<<<b->sms * 8, kBlock, 0, s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width,
+                                                     b->counters + kQueueCompose);
+  return check_launch("batch_compose_kernel");
+}
+
+int launch_trace_shade(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, int n_list, cudaStream_t s) {
+  if (int st = launch_trace(b, cfg, tiles, n_tiles, s)) return st;
+  return launch_shade(b, cfg, tiles, n_tiles, n_list, s);
+}
+
+// Rebuild the tile and view lists for cfg and capture setup -> trace ->
+// shadow -> compose -> filter.
 int configure(arbor_batch* b, const arbor_batch_config& cfg) {
   std::vector<int> all(b->n_views);
   std::iota(all.begin(), all.end(), 0);
   std::vector<int4> t;
-  trace_tiles(b, view_order(b, all, cfg.order), cfg.tile_width, t);
+  const std::vector<int> order = view_order(b, all, cfg.order);
+  trace_tiles(b, order, cfg.tile_width, t);
   const int n_ts = (int)t.size();
   filter_tiles(b, t);
   if (t.size() > b->tile_capacity) {
@@ -238,6 +316,7 @@ int configure(arbor_batch* b, const arbor_batch_config& cfg) {
   }
   BATCH_CUDA(cudaStreamSynchronize(b->own));
   BATCH_CUDA(cudaMemcpyAsync(b->tiles, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice, b->own));
+  BATCH_CUDA(cudaMemcpyAsync(b->vlist, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, b->own));
   BATCH_CUDA(cudaStreamSynchronize(b->own));
   b->n_ts = n_ts;
   b->n_filter = (int)t.size() - n_ts;
@@ -247,9 +326,10 @@ int configure(arbor_batch* b, const arbor_batch_config& cfg) {
   b->graph = nullptr;
   BATCH_CUDA(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
   int st = launch_setup(b, b->own);
-  if (!st) st = launch_trace_shade(b, cfg, b->tiles, b->n_ts, b->own);
+  if (!st) st = launch_trace_shade(b, cfg, b->tiles, b->n_ts, b->n_views, b->own);
   if (!st) {
-    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFY), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter, b->counters + 2);
+    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFY), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter,
+                                                                   b->counters + kQueueFilter);
     st = check_launch("batch_filter_kernel");
   }
   cudaGraph_t g = nullptr;
@@ -370,8 +450,8 @@ extern "C" int arbor_batch_create(arbor_batch** out, const int* seeds, int n_sce
   if ((ce = cudaEventCreateWithFlags(&b->joined, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_fail("cudaEventCreate", ce));
   if ((ce = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_fail("cudaEventCreate", ce));
   {
-    const void* kernels[] = {(const void*)batch_pass_kernel<4, false>, (const void*)batch_pass_kernel<4, true>,
-                             (const void*)batch_pass_kernel<8, false>, (const void*)batch_pass_kernel<8, true>};
+    const void* kernels[] = {(const void*)batch_pass_kernel<4>, (const void*)batch_shadow_kernel<4>, (const void*)batch_pass_kernel<8>,
+                             (const void*)batch_shadow_kernel<8>};
     const int bytes[] = {(int)batch_smem_bytes<4>(), (int)batch_smem_bytes<4>(), (int)batch_smem_bytes<8>(), (int)batch_smem_bytes<8>()};
     for (int k = 0; k < 4; k++)
       if ((ce = cudaFuncSetAttribute(kernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes[k])) != cudaSuccess)
@@ -390,7 +470,8 @@ extern "C" int arbor_batch_create(arbor_batch** out, const int* seeds, int n_sce
       {(void**)&b->cams, (size_t)n_views * sizeof(Camera)},
       {(void**)&b->scal, (size_t)n_views * sizeof(float4)},
       {(void**)&b->insts, (size_t)n_views * kForest * sizeof(Instance)},
-      {(void**)&b->counters, 3 * sizeof(int)},
+      {(void**)&b->counters, (size_t)(kViewQueues + n_views) * sizeof(int)},
+      {(void**)&b->vlist, (size_t)n_views * sizeof(int)},
       {(void**)&b->tiles, tiles * sizeof(int4)},
       {&b->scratch, arbor_sort_scratch_bytes()},
   };
@@ -476,7 +557,7 @@ extern "C" int arbor_batch_render(arbor_batch* b) {
   if (int s = live(b, "arbor_batch_render")) return s;
   if (int s = join_user(b)) return s;
   BATCH_CUDA(cudaGraphLaunch(b->exec, b->own));
-  count_launch(4);
+  count_launch(5);
   b->renders++;
   return join_back(b);
 }
@@ -487,13 +568,12 @@ extern "C" int arbor_batch_profile(arbor_batch* b, float* ms4) {
     set_error("arbor_batch_profile: ms4 is NULL");
     return ARBOR_ERR_NULL;
   }
-  // The graph's four kernels launched one by one, with an event between each.
+  // The graph's kernels launched one by one, with an event between the
+  // stages (the shade stage is the shadow and compose kernels).
   cudaEvent_t ev[5] = {};
   int status = ARBOR_OK;
   for (auto& e : ev)
     if (cudaEventCreate(&e) != cudaSuccess) status = cuda_fail("cudaEventCreate", cudaGetLastError());
-  const dim3 grid(b->sms * b->cfg.ctas_per_sm);
-  int* ctr = b->counters;
   if (status == ARBOR_OK) status = join_user(b);
   if (status == ARBOR_OK) {
     cudaEventRecord(ev[0], b->own);
@@ -501,32 +581,21 @@ extern "C" int arbor_batch_profile(arbor_batch* b, float* ms4) {
     cudaEventRecord(ev[1], b->own);
   }
   if (status == ARBOR_OK) {
-    if (b->cfg.queue == 4)
-      batch_pass_kernel<4, false><<<grid, kBlock, batch_smem_bytes<4>(), b->own>>>(b->views, b->cams, b->insts, b->tiles, b->n_ts,
-                                                                                   b->cfg.tile_width, ctr);
-    else
-      batch_pass_kernel<8, false><<<grid, kBlock, batch_smem_bytes<8>(), b->own>>>(b->views, b->cams, b->insts, b->tiles, b->n_ts,
-                                                                                   b->cfg.tile_width, ctr);
-    status = check_launch("batch_pass_kernel");
+    status = launch_trace(b, b->cfg, b->tiles, b->n_ts, b->own);
     cudaEventRecord(ev[2], b->own);
   }
   if (status == ARBOR_OK) {
-    if (b->cfg.queue == 4)
-      batch_pass_kernel<4, true><<<grid, kBlock, batch_smem_bytes<4>(), b->own>>>(b->views, b->cams, b->insts, b->tiles, b->n_ts,
-                                                                                  b->cfg.tile_width, ctr + 1);
-    else
-      batch_pass_kernel<8, true><<<grid, kBlock, batch_smem_bytes<8>(), b->own>>>(b->views, b->cams, b->insts, b->tiles, b->n_ts,
-                                                                                  b->cfg.tile_width, ctr + 1);
-    status = check_launch("batch_pass_kernel");
+    status = launch_shade(b, b->cfg, b->tiles, b->n_ts, b->n_views, b->own);
     cudaEventRecord(ev[3], b->own);
   }
   if (status == ARBOR_OK) {
-    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFY), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter, ctr + 2);
+    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFY), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter,
+                                                                   b->counters + kQueueFilter);
     status = check_launch("batch_filter_kernel");
     cudaEventRecord(ev[4], b->own);
   }
   if (status == ARBOR_OK) {
-    count_launch(4);
+    count_launch(5);
     cudaError_t ce = cudaEventSynchronize(ev[4]);
     if (ce != cudaSuccess) status = cuda_fail("cudaEventSynchronize", ce);
     for (int k = 0; k < 4 && status == ARBOR_OK; k++) cudaEventElapsedTime(&ms4[k], ev[k], ev[k + 1]);
@@ -556,18 +625,20 @@ extern "C" int arbor_batch_autotune(arbor_batch* b, int sample_views, arbor_batc
         for (int q : {4, 8}) {
           const arbor_batch_config cfg{tw, ctas, order, q};
           std::vector<int4> t;
-          trace_tiles(b, view_order(b, subset, order), tw, t);
+          const std::vector<int> vo = view_order(b, subset, order);
+          trace_tiles(b, vo, tw, t);
           float ms = 0.0f;
           if (status == ARBOR_OK) {
             // the previous candidate's kernels must be done with the tile list
             cudaError_t ce = cudaStreamSynchronize(b->own);
             if (ce == cudaSuccess) ce = cudaMemcpyAsync(b->tiles, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice, b->own);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(b->vlist, vo.data(), vo.size() * sizeof(int), cudaMemcpyHostToDevice, b->own);
             if (ce != cudaSuccess) status = cuda_fail("autotune tile upload", ce);
             // one untimed run, then one timed run
             for (int rep = 0; rep < 2 && status == ARBOR_OK; rep++) {
               if ((status = launch_setup(b, b->own))) break;
               if (rep == 1 && (ce = cudaEventRecord(e0, b->own)) != cudaSuccess) status = cuda_fail("cudaEventRecord", ce);
-              if (status || (status = launch_trace_shade(b, cfg, b->tiles, (int)t.size(), b->own))) break;
+              if (status || (status = launch_trace_shade(b, cfg, b->tiles, (int)t.size(), (int)vo.size(), b->own))) break;
               if (rep == 1 && (ce = cudaEventRecord(e1, b->own)) != cudaSuccess) status = cuda_fail("cudaEventRecord", ce);
             }
             if (status == ARBOR_OK) {
@@ -576,7 +647,7 @@ extern "C" int arbor_batch_autotune(arbor_batch* b, int sample_views, arbor_batc
               else
                 cudaEventElapsedTime(&ms, e0, e1);
             }
-            count_launch(6);
+            count_launch(8);  // two runs of setup, trace, shadow, compose
           }
           if (ms_table) ms_table[slot] = ms;
           slot++;
@@ -626,7 +697,7 @@ extern "C" int arbor_batch_inspect(arbor_batch* b, arbor_batch_info* info) {
   info->trace_tiles = b->n_ts;
   info->filter_tiles = b->n_filter;
   info->renders = b->renders;
-  info->launches_per_render = 4;
+  info->launches_per_render = 5;
   info->config = b->cfg;
   return ARBOR_OK;
 }
@@ -652,7 +723,7 @@ extern "C" int arbor_batch_destroy(arbor_batch* b) {
   if (b->own) cudaStreamSynchronize(b->own);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  void* bufs[] = {b->scenes, b->images, b->pixels, b->C, b->views, b->cams, b->scal, b->insts, b->counters, b->tiles, b->scratch};
+  void* bufs[] = {b->scenes, b->images, b->pixels, b->C, b->views, b->cams, b->scal, b->insts, b->counters, b->vlist, b->tiles, b->scratch};
   for (void* p : bufs)
     if (p) cudaFree(p);
   if (b->staging) cudaFreeHost(b->staging);

@@ -337,90 +337,6 @@ __device__ __forceinline__ f3 shade_post(const Shading& o, f3 visibility) {
   return mix3(col, o.skyc, o.haze);
 }
 
-// shadePixels in one pass, for the batched renderer's tiles: the surface
-// terms, then the shadow segments (Arbor.cu:271-274: at most four forest
-// traces toward the sun, 36 m, leaf transmission, any other hit opaque)
-// through the same warp-batched tracer; a pixel without a shadow ray
-// finishes when shaded.  (The single-image shadePixels runs the shadow
-// segments and the shading as separate passes; in the batch's tile kernel
-// that split measured slower than this fused form.)
-template <bool kForestScene>
-struct ShadePolicy {
-  const float* P;
-  float* Linear;
-  float* Guide;
-  const TraceCtx* ctx;
-  const Camera* cam;
-  const Instance* inst;
-  const float* Hit;
-  float* Normal;  // nullable: G-buffer normal output
-  int width, height;
-  int pixel, seg;
-  f3 trans;
-  Shading sh;
-  // Shade pixel (x, y): the surface terms, then the first shadow segment
-  // toward the sun, or the final colour when no visibility is needed.
-  __device__ __forceinline__ void start(const TraceCtx& c, Ray& r, int x, int y) {
-    pixel = y * width + x;
-    shade_pre<kForestScene>(P, *cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + pixel), x, y, width, height, sh);
-    if (!sh.final && sh.shadow) {
-      trans = mk(1.0f, 1.0f, 1.0f);
-      seg = 0;
-      ray_begin(c, r, sh.origin, sh.light, 36.0f);
-    } else {
-      write(mk(1.0f, 1.0f, 1.0f));
-      r.phase = kPhIdle;
-    }
-  }
-  __device__ __forceinline__ void write(f3 visibility) {
-    f3 col = shade_post(sh, visibility);
-    reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
-    reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);
-    if (Normal) reinterpret_cast<float4*>(Normal)[pixel] = make_float4(sh.normal.x, sh.normal.y, sh.normal.z, 0.0f);
-  }
-  __device__ __forceinline__ void done(Ray& r) {
-    int id = (int)r.found;
-    if (id < 0) {
-      write(trans);
-    } else if (ldg4(P, id * 6).w != 1.0f) {
-      write(mk(0.0f, 0.0f, 0.0f));
-    } else {
-      trans = trans * mk(0.18f, 0.29f, 0.065f);
-      sh.origin = sh.origin + sh.light * (r.best + 0.0018f);
-      if (++seg < 4) {
-        ray_begin(*ctx, r, sh.origin, sh.light, 36.0f);
-        return;
-      }
-      write(trans);
-    }
-    r.phase = kPhIdle;
-  }
-};
-
-// One tile of shadePixels (Arbor.cu:277-289); c is the shadow-ray context.
-template <bool kForestScene, class WB>
-__device__ __forceinline__ void shade_tile(const TraceCtx& c, const Camera& cam, const Instance* inst, WB& b, const float* __restrict__ P,
-                                           const float* __restrict__ Hit, float* __restrict__ Linear, float* __restrict__ Guide, int width,
-                                           int height, int x0, int y0, int tw, float* __restrict__ Normal = nullptr) {
-  int x, y;
-  tile_pixel_at(threadIdx.x, x0, y0, tw, x, y);
-  ShadePolicy<kForestScene> policy;
-  policy.Normal = Normal;
-  policy.P = P;
-  policy.Linear = Linear;
-  policy.Guide = Guide;
-  policy.ctx = &c;
-  policy.cam = &cam;
-  policy.inst = inst;
-  policy.Hit = Hit;
-  policy.width = width;
-  policy.height = height;
-  Ray r;
-  r.phase = kPhIdle;
-  if (x < width && y < height) policy.start(c, r, x, y);
-  batch_run(c, r, b, policy);
-}
-
 // The shadow ray of pixel (x, y), when shadePixels traces one: a surface hit
 // (not sky), no debug view, sun shadows on.  The same values shade_pre
 // computes for the pixel.

@@ -294,13 +294,44 @@ __device__ __forceinline__ bool pool_take(const PixelPool& pool, unsigned idle, 
   return got;
 }
 
+// The pixels of one image shared by every CTA that works on it: its 8x4
+// blocks 0, 1, 2, ... handed out one pixel at a time from a counter in
+// global memory (the batched renderer's per-view pools).
+struct ViewPool {
+  int* next;  // global counter of pixels handed out for this image
+  int width, height, blocks_x, blocks;
+};
+
+// ViewPool form of pool_take (same contract).
+__device__ __forceinline__ bool pool_take(const ViewPool& pool, unsigned idle, int lane, int& x, int& y, bool& past) {
+  const unsigned full = 0xffffffffu;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(pool.next, __popc(idle));
+  base = __shfl_sync(full, base, 0);
+  bool got = false, beyond = false;
+  if (idle & (1u << lane)) {
+    const int idx = base + __popc(idle & ((1u << lane) - 1u));
+    const int block = idx >> 5;
+    if (block >= pool.blocks) {
+      beyond = true;
+    } else {
+      const int by = block / pool.blocks_x, bx = block - by * pool.blocks_x;
+      x = bx * 8 + (idx & 7);
+      y = by * 4 + ((idx >> 3) & 3);
+      got = x < pool.width && y < pool.height;
+    }
+  }
+  past = __any_sync(full, beyond);
+  return got;
+}
+
 // Drive one warp through a pixel pool: lanes whose rays are finished take
 // the next pixels (Policy::start begins a ray, or finishes the pixel at
 // once), so no lane waits for the slowest ray of a fixed tile.  Policy::done
 // is called for a finished ray and either continues it (a new trace on r) or
 // sets it idle.
-template <class WB, class Policy>
-__device__ __forceinline__ void batch_run_pool(const TraceCtx& c, Ray& r, WB& b, Policy& policy, const PixelPool& pool) {
+template <class WB, class Policy, class Pool>
+__device__ __forceinline__ void batch_run_pool(const TraceCtx& c, Ray& r, WB& b, Policy& policy, const Pool& pool) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   int nq = 0;

@@ -331,9 +331,9 @@ ARBOR_API int arbor_batch_get_config(arbor_batch* b, arbor_batch_config* cfg);
 ARBOR_API int arbor_batch_autotune(arbor_batch* b, int sample_views, arbor_batch_config* best, float* ms_table);
 /* Renders every view: one graph launch. */
 ARBOR_API int arbor_batch_render(arbor_batch* b);
-/* Renders every view with the graph's four kernels launched one by one and
- * writes each one's duration (CUDA events, ms) to ms4: setup, trace, shade,
- * filter+resolve. */
+/* Renders every view with the graph's kernels launched one by one and writes
+ * each stage's duration (CUDA events, ms) to ms4: setup, trace, shade (the
+ * shadow and compose kernels), filter+resolve. */
 ARBOR_API int arbor_batch_profile(arbor_batch* b, float* ms4);
 /* Device buffers of one view (its scene's records, its C record and images). */
 ARBOR_API int arbor_batch_view_buffers(arbor_batch* b, int view, arbor_engine_buffers* out);

@@ -163,7 +163,7 @@ def test_batch_set_cameras_and_pixels(cuda, gu, batch, singles):
     batch.call("arbor_batch_render")
     info = ab.BatchInfo()
     batch.call("arbor_batch_inspect", ctypes.byref(info))
-    assert info.n_views == len(SIZES) and info.n_scenes == len(SEEDS) and info.launches_per_render == 4
+    assert info.n_views == len(SIZES) and info.n_scenes == len(SEEDS) and info.launches_per_render == 5
     assert info.total_pixels == sum(w * h for w, h in SIZES)
     px = np.zeros(info.total_pixels, np.uint32)
     batch.call("arbor_batch_read_pixels", px.ctypes.data_as(ctypes.c_void_p), px.size)
