@@ -6,14 +6,14 @@
 //   batch_setup_kernel        per view: camera constants, the forest
 //                             instance table and the filter/resolve scalars
 //                             of its C record; resets the queues
-//   batch_pass_kernel         persistent CTAs pull tiles of every view from
-//                             one global queue and run tracePixels
-//                             (Arbor.cu:252) on each
-//   batch_shadow_kernel       persistent warps walk the views; in each, their
-//                             lanes take pixels from the view's own queue
-//                             as their rays finish and trace the shadow
-//                             segments of shadePixels (Arbor.cu:271-274)
-//   batch_compose_kernel      the trace tiles again: shadePixels' colours
+//   batch_pool_kernel<trace>  persistent warps walk the views; in each, their
+//                             lanes take pixels from the view's own queue as
+//                             their rays finish and run tracePixels
+//                             (Arbor.cu:252)
+//   batch_pool_kernel<shadow> the same for the shadow segments of
+//                             shadePixels (Arbor.cu:271-274)
+//   batch_compose_kernel      persistent CTAs pull tiles of every view from
+//                             one global queue: shadePixels' colours
 //                             (Arbor.cu:277-289) with that visibility
 //   batch_filter_kernel       persistent CTAs pull 32x8 tiles and run the
 //                             fused filterLighting + resolvePixels
@@ -26,8 +26,8 @@
 // met (the warp batch groups rays by tile; see warpbatch.cuh).
 //
 // The autotuner times the trace, shadow and compose kernels on a sample of
-// the views for each tile shape (16x16 or 32x8), CTAs per SM (1 or 2), tile
-// order (view by view, or the largest views first) and warp-batch queue
+// the views for each compose tile shape (16x16 or 32x8), CTAs per SM (1 or
+// 2), view order (as given, or the largest views first) and warp-batch queue
 // depth (4 or 8 candidates per lane), and keeps the fastest.
 #include <algorithm>
 #include <cstring>
@@ -41,9 +41,10 @@
 namespace arbor {
 namespace {
 
-// Work queues (global counters) of one render: the trace tiles, the compose
-// tiles, the filter tiles, then one pixel queue per view for the shadow pass.
-constexpr int kQueueTrace = 0, kQueueCompose = 1, kQueueFilter = 2, kViewQueues = 3;
+// Work queues (global counters) of one render: the compose tiles, the filter
+// tiles, then one pixel queue per view for the trace pass and one per view
+// for the shadow pass.
+constexpr int kQueueCompose = 0, kQueueFilter = 1, kViewQueues = 2;
 
 struct BatchView {
   const float* P;
@@ -61,7 +62,10 @@ struct BatchView {
 __global__ void __launch_bounds__(kBlock) batch_setup_kernel(const float* __restrict__ Cs, Camera* __restrict__ cams, float4* __restrict__ scal,
                                                              Instance* __restrict__ insts, int* __restrict__ counters) {
   const int v = blockIdx.x;
-  if (threadIdx.x == 0) counters[kViewQueues + v] = 0;
+  if (threadIdx.x == 0) {
+    counters[kViewQueues + v] = 0;
+    counters[kViewQueues + gridDim.x + v] = 0;
+  }
   const float* C = Cs + v * 64;
   if (threadIdx.x == 0) {
     Camera cam;
@@ -74,61 +78,36 @@ __global__ void __launch_bounds__(kBlock) batch_setup_kernel(const float* __rest
   if (v == 0 && threadIdx.x < kViewQueues) counters[threadIdx.x] = 0;
 }
 
-// tracePixels of each tile.  The shade runs as separate kernels: their
-// register allocation and code stay out of the trace's loop.
-template <int Q>
-__global__ void __launch_bounds__(kBlock, 2) batch_pass_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
-                                                               const Instance* __restrict__ insts, const int4* __restrict__ tiles,
-                                                               int n_tiles, int tw, int* __restrict__ counter) {
-  using WB = WarpBatchQ<Q>;
-  extern __shared__ float4 batch_smem[];
-  WB& b = reinterpret_cast<WB*>(batch_smem)[threadIdx.x >> 5];
-  __shared__ Camera cam;
-  __shared__ Instance inst[kForest];
-  __shared__ int s_tile;
-  int cur = -1;
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = s_tile;
-    if (t >= n_tiles) break;
-    const int4 td = __ldg(tiles + t);
-    if (td.x != cur) {  // uniform across the CTA
-      cur = td.x;
-      if (threadIdx.x == 0) cam = cams[cur];
-      for (int k = threadIdx.x; k < kForest; k += blockDim.x) inst[k] = insts[cur * kForest + k];
-      __syncthreads();
-    }
-    const BatchView v = views[cur];
-    const TraceCtx c{v.P, v.Nodes, v.Order, inst, cam.c14 / (float)v.height, cam.time, cam.wind, true, true};
-    trace_tile(c, cam, b, v.Hit, v.width, v.height, td.y, td.z, tw);
-    __syncthreads();  // every thread has read s_tile, cam and inst
-  }
-}
-
-// The shadow segments of every view (visibility into its Linear image).
-// Each warp walks the views in order and joins each one's pixel queue; its
-// lanes take the view's next pixels as their rays finish, so warps of any
-// CTA share a view's work and move on independently.  The view's camera and
-// instance table are read from global memory (the same values setup wrote).
-template <int Q>
-__global__ void __launch_bounds__(kBlock, 2) batch_shadow_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
-                                                                 const Instance* __restrict__ insts, const int* __restrict__ list, int n_list,
-                                                                 int* __restrict__ queues) {
+// tracePixels (kShadow false) or the shadow segments of shadePixels (true,
+// visibility into Linear) of every listed view.  Each warp walks the views in
+// order and joins each one's pixel queue; its lanes take the view's next
+// pixels as their rays finish, so warps of any CTA share a view's work and
+// move on independently.  The view's camera and instance table are read from
+// global memory (the values setup wrote).
+template <int Q, bool kShadow>
+__global__ void __launch_bounds__(kBlock, 2) batch_pool_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
+                                                               const Instance* __restrict__ insts, const int* __restrict__ list, int n_list,
+                                                               int* __restrict__ queues) {
   using WB = WarpBatchQ<Q>;
   extern __shared__ float4 batch_smem[];
   WB& b = reinterpret_cast<WB*>(batch_smem)[threadIdx.x >> 5];
   for (int i = 0; i < n_list; i++) {
     const int v = __ldg(list + i);
     const Camera& cam = cams[v];
-    if (!(cam.shadows > 0.5f)) continue;
+    if (kShadow && !(cam.shadows > 0.5f)) continue;
     const BatchView view = views[v];
-    const TraceCtx c{view.P, view.Nodes, view.Order, insts + (size_t)v * kForest, 0.0001f, cam.time, cam.wind, false, true};
     const int bx = (view.width + 7) / 8;
     const ViewPool pool{queues + v, view.width, view.height, bx, bx * ((view.height + 3) / 4)};
-    ShadowPolicy policy{&c, &cam, view.Hit, view.Linear, view.width, view.height, 0, 0};
     Ray r;
-    batch_run_pool(c, r, b, policy, pool);
+    if (kShadow) {
+      const TraceCtx c{view.P, view.Nodes, view.Order, insts + (size_t)v * kForest, 0.0001f, cam.time, cam.wind, false, true};
+      ShadowPolicy policy{&c, &cam, view.Hit, view.Linear, view.width, view.height, 0, 0};
+      batch_run_pool(c, r, b, policy, pool);
+    } else {
+      const TraceCtx c{view.P, view.Nodes, view.Order, insts + (size_t)v * kForest, cam.c14 / (float)view.height, cam.time, cam.wind, true, true};
+      PrimaryPolicy policy{&cam, view.Hit, view.width, view.height, 0};
+      batch_run_pool(c, r, b, policy, pool);
+    }
   }
 }
 
@@ -227,7 +206,7 @@ struct arbor_batch {
   Camera* cams = nullptr;
   float4* scal = nullptr;
   Instance* insts = nullptr;
-  int* counters = nullptr;     // work queues: kViewQueues tile queues, then one pixel queue per view
+  int* counters = nullptr;     // work queues: kViewQueues tile queues, then 2 pixel queues per view
   int* vlist = nullptr;        // views the shadow pass walks, in order
   int4* tiles = nullptr;       // trace/shade tiles, then filter tiles
   int n_ts = 0, n_filter = 0;
@@ -269,34 +248,34 @@ int launch_setup(arbor_batch* b, cudaStream_t s) {
   return check_launch("batch_setup_kernel");
 }
 
-// The trace pass over the tile list.
-int launch_trace(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, cudaStream_t s) {
+// The trace pass over the listed views.
+int launch_trace(arbor_batch* b, const arbor_batch_config& cfg, int n_list, cudaStream_t s) {
   const dim3 grid(b->sms * cfg.ctas_per_sm);
-  int* ctr = b->counters + kQueueTrace;
+  int* queues = b->counters + kViewQueues;
   if (cfg.queue == 4)
-    batch_pass_kernel<4><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr);
+    batch_pool_kernel<4, false><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
   else
-    batch_pass_kernel<8><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width, ctr);
-  return check_launch("batch_pass_kernel");
+    batch_pool_kernel<8, false><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
+  return check_launch("batch_pool_kernel");
 }
 
 // shadePixels: the shadow pass over the listed views, then the compose pass
 // over the tile list.
 int launch_shade(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, int n_list, cudaStream_t s) {
   const dim3 grid(b->sms * cfg.ctas_per_sm);
-  int* queues = b->counters + kViewQueues;
+  int* queues = b->counters + kViewQueues + b->n_views;
   if (cfg.queue == 4)
-    batch_shadow_kernel<4><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
+    batch_pool_kernel<4, true><<<grid, kBlock, batch_smem_bytes<4>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
   else
-    batch_shadow_kernel<8><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
-  if (int st = check_launch("batch_shadow_kernel")) return st;
+    batch_pool_kernel<8, true><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
+  if (int st = check_launch("batch_pool_kernel")) return st;
   batch_compose_kernel<<<b->sms * 8, kBlock, 0, s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width,
                                                      b->counters + kQueueCompose);
   return check_launch("batch_compose_kernel");
 }
 
 int launch_trace_shade(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, int n_list, cudaStream_t s) {
-  if (int st = launch_trace(b, cfg, tiles, n_tiles, s)) return st;
+  if (int st = launch_trace(b, cfg, n_list, s)) return st;
   return launch_shade(b, cfg, tiles, n_tiles, n_list, s);
 }
 
@@ -450,8 +429,8 @@ extern "C" int arbor_batch_create(arbor_batch** out, const int* seeds, int n_sce
   if ((ce = cudaEventCreateWithFlags(&b->joined, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_fail("cudaEventCreate", ce));
   if ((ce = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_fail("cudaEventCreate", ce));
   {
-    const void* kernels[] = {(const void*)batch_pass_kernel<4>, (const void*)batch_shadow_kernel<4>, (const void*)batch_pass_kernel<8>,
-                             (const void*)batch_shadow_kernel<8>};
+    const void* kernels[] = {(const void*)batch_pool_kernel<4, false>, (const void*)batch_pool_kernel<4, true>,
+                             (const void*)batch_pool_kernel<8, false>, (const void*)batch_pool_kernel<8, true>};
     const int bytes[] = {(int)batch_smem_bytes<4>(), (int)batch_smem_bytes<4>(), (int)batch_smem_bytes<8>(), (int)batch_smem_bytes<8>()};
     for (int k = 0; k < 4; k++)
       if ((ce = cudaFuncSetAttribute(kernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes[k])) != cudaSuccess)
@@ -470,7 +449,7 @@ extern "C" int arbor_batch_create(arbor_batch** out, const int* seeds, int n_sce
       {(void**)&b->cams, (size_t)n_views * sizeof(Camera)},
       {(void**)&b->scal, (size_t)n_views * sizeof(float4)},
       {(void**)&b->insts, (size_t)n_views * kForest * sizeof(Instance)},
-      {(void**)&b->counters, (size_t)(kViewQueues + n_views) * sizeof(int)},
+      {(void**)&b->counters, (size_t)(kViewQueues + 2 * n_views) * sizeof(int)},
       {(void**)&b->vlist, (size_t)n_views * sizeof(int)},
       {(void**)&b->tiles, tiles * sizeof(int4)},
       {&b->scratch, arbor_sort_scratch_bytes()},
@@ -581,7 +560,7 @@ extern "C" int arbor_batch_profile(arbor_batch* b, float* ms4) {
     cudaEventRecord(ev[1], b->own);
   }
   if (status == ARBOR_OK) {
-    status = launch_trace(b, b->cfg, b->tiles, b->n_ts, b->own);
+    status = launch_trace(b, b->cfg, b->n_views, b->own);
     cudaEventRecord(ev[2], b->own);
   }
   if (status == ARBOR_OK) {

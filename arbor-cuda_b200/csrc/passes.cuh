@@ -17,8 +17,8 @@ __device__ __forceinline__ void tile_pixel_at(int t, int x0, int y0, int tw, int
 }
 
 // ---------------------------------------------------------------- trace --
-// One ray per thread over 16x16-pixel CTAs (8x4-pixel warps); each warp's
-// primitive tests run warp-batched (warpbatch.cuh).
+// Primary rays (tracePixels); each warp's primitive tests run warp-batched
+// (warpbatch.cuh).
 struct PrimaryPolicy {
   static constexpr int kRefill = 8;  // idle lanes that trigger a refill (measured best of 1-16)
   const Camera* cam;
@@ -37,19 +37,6 @@ struct PrimaryPolicy {
     r.phase = kPhIdle;
   }
 };
-
-// Primary rays of one tile (tracePixels, Arbor.cu:252).
-template <class WB>
-__device__ __forceinline__ void trace_tile(const TraceCtx& c, const Camera& cam, WB& b, float* __restrict__ Hit, int width, int height,
-                                           int x0, int y0, int tw) {
-  int x, y;
-  tile_pixel_at(threadIdx.x, x0, y0, tw, x, y);
-  PrimaryPolicy policy{&cam, Hit, width, height, y * width + x};
-  Ray r;
-  r.phase = kPhIdle;
-  if (x < width && y < height) policy.start(c, r, x, y);
-  batch_run(c, r, b, policy);
-}
 
 // Primary rays of every pixel of a persistent CTA's pool.
 template <class WB>

@@ -296,9 +296,9 @@ typedef struct arbor_batch_view {
 } arbor_batch_view;
 
 typedef struct arbor_batch_config {
-  int tile_width;   /* trace/shade tile: 16 (16x16 pixels) or 32 (32x8 pixels) */
+  int tile_width;   /* shading (compose) tile: 16 (16x16 pixels) or 32 (32x8 pixels) */
   int ctas_per_sm;  /* persistent CTAs per SM: 1 or 2 */
-  int order;        /* tile order: 0 view by view, 1 largest views first */
+  int order;        /* view order of every pass: 0 as given, 1 largest views first */
   int queue;        /* warp-batch queue depth, candidates per lane: 4 or 8 */
 } arbor_batch_config;
 
@@ -322,7 +322,7 @@ ARBOR_API int arbor_batch_create(arbor_batch** out, const int* seeds, int n_scen
 ARBOR_API int arbor_batch_set_cameras(arbor_batch* b, const float* C, int n_views);
 ARBOR_API int arbor_batch_configure(arbor_batch* b, const arbor_batch_config* cfg);
 ARBOR_API int arbor_batch_get_config(arbor_batch* b, arbor_batch_config* cfg);
-/* Times the trace and shade kernels of every configuration (16, ordered by
+/* Times the trace, shadow and compose kernels of every configuration (16, ordered by
  * tile_width, ctas_per_sm, order, queue, the last varying fastest) on
  * `sample_views` views spread over the batch (all when <= 0), writes the
  * times to ms_table (nullable, 16 floats), keeps the fastest and returns it
