@@ -72,6 +72,74 @@ __global__ void __launch_bounds__(kBlock) shade_compose_kernel(const float* __re
   if (x < width && y < height) shade_compose_px<kForestScene>(P, cam, inst, Hit, Linear, Guide, Normal, x, y, width, height);
 }
 
+// tracePixels and shadePixels with the reference's traversal as written
+// (Arbor.cu:220-289): one ray per thread over 16x16-pixel CTAs, candidates
+// tested in visiting order, children nearest entry first, no warp batching.
+// Slower forms kept to check that the batched passes' order does not change
+// a result (the in-order entry points).
+template <bool kForestScene>
+__global__ void __launch_bounds__(kBlock) trace_inorder_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                               const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                               float* __restrict__ Hit, int width, int height) {
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForestScene ? kForest : 1];
+  block_setup(C, cam, inst, kForestScene);
+  int x, y;
+  tile_pixel(threadIdx.x, x, y);
+  if (x >= width || y >= height) return;
+  const f3 ro = cam.ro;
+  const f3 rd = camera_ray(cam, x, y, width, height);
+  const float ground = rd.y < -0.00001f ? -ro.y / rd.y : kFar;
+  const float cone = cam.c14 / (float)height;
+  const float best = ground > 0.0f ? ground : kFar;
+  int tree = -1;
+  const f2 h = kForestScene ? trace_forest(P, Nodes, Order, inst, ro, rd, cone, cam.time, cam.wind, best, &tree, false)
+                            : trace_tree(P, Nodes, Order, ro, rd, cone, cam.time, cam.wind, best, -1, false);
+  reinterpret_cast<float4*>(Hit)[y * width + x] = make_float4(h.x, h.y, (float)tree, cam.c14 * h.x / (float)height);
+}
+
+template <bool kForestScene>
+__global__ void __launch_bounds__(kBlock) shade_inorder_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                               const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                               const float* __restrict__ Hit, float* __restrict__ Linear,
+                                                               float* __restrict__ Guide, int width, int height) {
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForestScene ? kForest : 1];
+  block_setup(C, cam, inst, kForestScene);
+  int x, y;
+  tile_pixel(threadIdx.x, x, y);
+  if (x >= width || y >= height) return;
+  const int pixel = y * width + x;
+  Shading sh;
+  shade_pre<kForestScene>(P, cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + pixel), x, y, width, height, sh);
+  f3 vis = mk(1.0f, 1.0f, 1.0f);
+  if (!sh.final && sh.shadow) {
+    // lightVisibility (Arbor.cu:271-274)
+    f3 trans = mk(1.0f, 1.0f, 1.0f);
+    f3 o = sh.origin;
+    for (int j = 0; j < 4; j++) {
+      int tree = -1;
+      const f2 h = kForestScene ? trace_forest(P, Nodes, Order, inst, o, sh.light, 0.0001f, cam.time, cam.wind, 36.0f, &tree, true)
+                                : trace_tree(P, Nodes, Order, o, sh.light, 0.0001f, cam.time, cam.wind, 36.0f, -1, true);
+      const int id = (int)h.y;
+      if (id < 0) {
+        vis = trans;
+        break;
+      }
+      if (ldg4(P, id * 6).w != 1.0f) {
+        vis = mk(0.0f, 0.0f, 0.0f);
+        break;
+      }
+      trans = trans * mk(0.18f, 0.29f, 0.065f);
+      o = o + sh.light * (h.x + 0.0018f);
+      if (j == 3) vis = trans;
+    }
+  }
+  const f3 col = shade_post(sh, vis);
+  reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
+  reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);
+}
+
 template <bool kResolve>
 __global__ void __launch_bounds__(kFX * kFY) filter_kernel(const float* __restrict__ Linear, const float* __restrict__ Guide,
                                                            const float* __restrict__ Hit, float* __restrict__ Filtered,
@@ -208,6 +276,43 @@ extern "C" int arbor_shadeGBuffer(const float* P, const float* Nodes, const uint
 extern "C" int arbor_shadeTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear,
                                      float* Guide, int width, int height, arbor_stream stream) {
   return shade_entry("arbor_shadeTreePixels", false, P, Nodes, Order, C, Hit, Linear, Guide, width, height, stream);
+}
+extern "C" int arbor_tracePixelsInOrder(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width,
+                                        int height, int single_tree, arbor_stream stream) {
+  const char* name = "arbor_tracePixelsInOrder";
+  bool empty;
+  if (int s = check_image(name, width, height, &empty)) return s;
+  const Binding b[] = {{P, kP, false, 16, "P"},
+                       {Nodes, kNodes, false, 16, "Nodes"},
+                       {Order, kKeys, false, 4, "Order"},
+                       {C, kC, false, 4, "C"},
+                       {Hit, empty ? 0 : image_bytes(width, height), true, 16, "Hit"}};
+  if (int s = check_bindings(name, b)) return s;
+  if (empty) return ARBOR_OK;
+  if (single_tree)
+    trace_inorder_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+  else
+    trace_inorder_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+  count_launch();
+  return check_launch(name);
+}
+extern "C" int arbor_shadePixelsInOrder(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit,
+                                        float* Linear, float* Guide, int width, int height, int single_tree, arbor_stream stream) {
+  const char* name = "arbor_shadePixelsInOrder";
+  bool empty;
+  if (int s = check_image(name, width, height, &empty)) return s;
+  size_t img = empty ? 0 : image_bytes(width, height);
+  const Binding b[] = {{P, kP, false, 16, "P"},         {Nodes, kNodes, false, 16, "Nodes"}, {Order, kKeys, false, 4, "Order"},
+                       {C, kC, false, 4, "C"},          {Hit, img, false, 16, "Hit"},        {Linear, img, true, 16, "Linear"},
+                       {Guide, img, true, 16, "Guide"}};
+  if (int s = check_bindings(name, b)) return s;
+  if (empty) return ARBOR_OK;
+  if (single_tree)
+    shade_inorder_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+  else
+    shade_inorder_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+  count_launch();
+  return check_launch(name);
 }
 extern "C" int arbor_filterLighting(const float* Linear, const float* Guide, const float* Hit, float* Filtered, const float* C, int width,
                                     int height, arbor_stream stream) {

@@ -190,6 +190,15 @@ ARBOR_API int arbor_buildScene(int seed, float* B, float* P, uint32_t* Keys, uin
  * normal, no per-tree tint, and shadow rays through the same tree. */
 ARBOR_API int arbor_traceTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height, arbor_stream stream);
 ARBOR_API int arbor_shadeTreePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, arbor_stream stream);
+/* tracePixels / shadePixels (single_tree = 0) or their single-tree forms
+ * (single_tree != 0) with the reference's traversal as written: one ray per
+ * thread, candidate primitives tested in visiting order, children nearest
+ * entry first (Arbor.cu:220-289).  Same buffers and results as the entries
+ * above; slower.  They exist to check that the batched passes' visiting
+ * order does not change a result.  No counterpart in the reference (which
+ * has only this order). */
+ARBOR_API int arbor_tracePixelsInOrder(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height, int single_tree, arbor_stream stream);
+ARBOR_API int arbor_shadePixelsInOrder(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, int single_tree, arbor_stream stream);
 
 /* shadePixels (Arbor.cu:277-289) that also writes the shading normal of
  * each pixel (world space, facing the camera; zero for sky) into Normal
