@@ -214,6 +214,12 @@ def workload_state(C: np.ndarray, spec: dict) -> np.ndarray:
     return C
 
 
+# Algorithmic bytes of one scene build: makeKeys 32768 x (96 + 8), the sort
+# 16 B per element per pass x 4 passes, makeBounds 32768 x (4 + 96 + 32),
+# the reduce levels 32767 x 96 (Arbor.cu:139-142).
+BUILD_BYTES = 32768 * (96 + 8) + 16 * 32768 * 4 + 32768 * (4 + 96 + 32) + 32767 * 96
+
+
 def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
     """The slowest rank's time (every rank calls it; a no-op for one rank)."""
     import torch
@@ -321,6 +327,12 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
         "roofline_hbm": {"kernel": "filterResolve", "bound": "hbm", "achieved": round(fr_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(fr_gbs / hbm_peak, 4) if hbm_peak else None, "traffic": None,
                          "algorithmic_bytes": fr_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "roofline_build": {"kernel": "buildScene (growth, primitives + keys, 4 radix passes, bounds)", "bound": "hbm",
+                           "achieved": round(BUILD_BYTES / (ms_build / 1e3) / 1e9, 1), "peak": hbm_peak, "unit": "GB/s",
+                           "frac": round(BUILD_BYTES / (ms_build / 1e3) / 1e9 / hbm_peak, 4) if hbm_peak else None, "traffic": None,
+                           "algorithmic_bytes": BUILD_BYTES, "ms_per_build": round(ms_build, 4),
+                           "note": "13 MB over a few dependent launches of a few thousand threads: launch- and latency-bound, far "
+                                   "from the HBM roof", "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
