@@ -156,6 +156,7 @@ def main() -> None:
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--scenes", type=int, default=16)
+    ap.add_argument("--hflip", action="store_true", help="add the mirrored training views (horizontal flip) to the training set")
     ap.add_argument("--out", default="")
     args = ap.parse_args()
     torch.cuda.init()
@@ -181,6 +182,15 @@ def main() -> None:
         r = render_pair(fr, scene_of(k), C, args.spp, eval_baselines=False)
         feats[i], base[i], target[i] = r["feat"], r["base"], r["target"]
     evals = [render_pair(fr, scene_of(k), C, args.spp, eval_baselines=True) | {"C": C} for k, C in eval_views]
+    n_train = args.train_views
+    if args.hflip:
+        # mirrored copies (every channel keeps its meaning; only the image's
+        # x axis is reversed), appended so batches of consecutive views stay
+        # within one half
+        feats = torch.cat([feats, feats.view(n_train, S, S, 16).flip(2).reshape(n_train, -1)])
+        base = torch.cat([base, base.view(n_train, S, S, 4).flip(2).reshape(n_train, -1)])
+        target = torch.cat([target, target.view(n_train, S, S, 4).flip(2).reshape(n_train, -1)])
+        n_train *= 2
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
 
@@ -191,7 +201,7 @@ def main() -> None:
     losses = []
     t0 = time.perf_counter()
     for step in range(args.steps):
-        i = int(rng.integers(0, args.train_views - args.batch + 1))
+        i = int(rng.integers(0, n_train - args.batch + 1))
         lr = 1e-5 + 0.5 * (args.lr - 1e-5) * (1.0 + math.cos(math.pi * step / args.steps))
         lv = ctypes.c_float()
         want = step % 50 == 0 or step == args.steps - 1
@@ -241,7 +251,7 @@ def main() -> None:
     result = {
         "denoiser": "4-level U-Net 32/64/96/128, 3x3, BF16 weights and activations, FP32 accumulation; forward "
                     "convolutions on tcgen05 (TMEM accumulators), backward on mma.sync m16n8k16",
-        "data": {"train_views": args.train_views, "eval_views": args.eval_views, "size": S, "spp_target": args.spp, "scenes": args.scenes,
+        "data": {"train_views": args.train_views, "eval_views": args.eval_views, "size": S, "spp_target": args.spp, "scenes": args.scenes, "hflip": bool(args.hflip),
                  "render_seconds": round(t_data, 1)},
         "train": {"steps": args.steps, "batch": args.batch, "lr": args.lr, "seconds": round(t_train, 2),
                   "ms_per_step": round(1e3 * t_train / max(1, args.steps), 3), "loss": losses},
