@@ -183,3 +183,18 @@ def test_image_files(lib, tmp_path):
     assert np.array_equal(body[::-1], img.reshape(h, w, 4)[..., :3])
     assert lib.arbor_write_ppm(None, px.ctypes.data, w, h) == ab.ERR_NULL
     assert lib.arbor_write_ppm(str(ppm).encode(), px.ctypes.data, 0, h) == ab.ERR_VALUE
+
+
+def test_in_order_entries_validate_like_the_batched_ones(lib):
+    """The in-order trace/shade take tracePixels'/shadePixels' buffers and
+    reject the same bad bindings before any launch."""
+    args = (A, A + 4 * MB, A + 8 * MB, A + 9 * MB, A + 16 * MB)
+    assert lib.arbor_tracePixelsInOrder(None, *args[1:], 64, 64, 0, None) == ab.ERR_NULL
+    assert lib.arbor_tracePixelsInOrder(A + 4, *args[1:], 64, 64, 0, None) == ab.ERR_ALIGN
+    assert lib.arbor_tracePixelsInOrder(A, A + 4 * MB, A + 8 * MB, A + 9 * MB, A + 64, 64, 64, 0, None) == ab.ERR_ALIAS
+    assert lib.arbor_tracePixelsInOrder(*args, -1, 64, 0, None) == ab.ERR_VALUE
+    assert lib.arbor_tracePixelsInOrder(*args, 64, 0, 1, None) == ab.OK  # zero workgroups: no-op
+    shade = (A, A + 4 * MB, A + 8 * MB, A + 9 * MB, A + 16 * MB, A + 32 * MB, A + 48 * MB)
+    assert lib.arbor_shadePixelsInOrder(*shade[:6], None, 64, 64, 0, None) == ab.ERR_NULL
+    assert lib.arbor_shadePixelsInOrder(*shade[:5], A + 32 * MB, A + 32 * MB, 64, 64, 0, None) == ab.ERR_ALIAS
+    assert lib.arbor_shadePixelsInOrder(*shade, 64, 0, 0, None) == ab.OK
