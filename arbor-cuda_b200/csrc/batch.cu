@@ -111,9 +111,9 @@ __global__ void __launch_bounds__(kBlock, 2) batch_pool_kernel(const BatchView* 
   }
 }
 
-// shadePixels' colours of each trace tile, one pixel per thread, with the
-// shadow pass's visibility.
-__global__ void __launch_bounds__(kBlock) batch_compose_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
+// shadePixels' colours of each tile, one pixel per thread, with the shadow
+// pass's visibility (4 CTAs per SM, as the single-image compose pass).
+__global__ void __launch_bounds__(kBlock, 4) batch_compose_kernel(const BatchView* __restrict__ views, const Camera* __restrict__ cams,
                                                                const Instance* __restrict__ insts, const int4* __restrict__ tiles,
                                                                int n_tiles, int tw, int* __restrict__ counter) {
   __shared__ Camera cam;
