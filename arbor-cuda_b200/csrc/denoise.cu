@@ -1427,6 +1427,37 @@ extern "C" int arbor_denoiser_train_step(arbor_denoiser* d, const uint16_t* feat
   return ARBOR_OK;
 }
 
+extern "C" int arbor_denoiser_gradient(arbor_denoiser* d, const uint16_t* features, const float* base, const float* target, int batch,
+                                       int width, int height, float* grad, size_t count, float* loss) {
+  if (int s = live(d, "arbor_denoiser_gradient")) return s;
+  if (features == nullptr || base == nullptr || target == nullptr || grad == nullptr) {
+    set_error("arbor_denoiser_gradient: features, base, target and grad must not be NULL");
+    return ARBOR_ERR_NULL;
+  }
+  if (count < (size_t)d->param_count) {
+    set_error("arbor_denoiser_gradient: need room for %ld floats", d->param_count);
+    return ARBOR_ERR_LIMIT;
+  }
+  if (int s = check_size("arbor_denoiser_gradient", batch, width, height, d)) return s;
+  cudaStream_t s = d->stream;
+  const bf16* f = reinterpret_cast<const bf16*>(features);
+  if (int st = forward(d, f, batch, width, height)) return st;
+  const long px = (long)batch * width * height;
+  DN_CUDA(cudaMemsetAsync(d->loss, 0, 4, s));
+  loss_kernel<<<ew_grid(px), 256, 0, s>>>(d->out, reinterpret_cast<const float4*>(base), reinterpret_cast<const float4*>(target), d->dout,
+                                          d->loss, px, 1.0f / (float)(px * 3));
+  count_launch();
+  if (int st = check_launch("loss_kernel")) return st;
+  if (int st = backward(d, f, batch, width, height)) return st;
+  DN_CUDA(cudaMemcpyAsync(grad, d->g, (size_t)d->param_count * 4, cudaMemcpyDeviceToHost, s));
+  DN_CUDA(cudaMemcpyAsync(&d->loss_host, d->loss, 4, cudaMemcpyDeviceToHost, s));
+  // the gradient buffer starts the next step at zero, as after an Adam step
+  DN_CUDA(cudaMemsetAsync(d->g, 0, (size_t)d->param_count * 4, s));
+  DN_CUDA(cudaStreamSynchronize(s));
+  if (loss) *loss = d->loss_host / (float)(px * 3);
+  return check_err(d, "arbor_denoiser_gradient");
+}
+
 extern "C" int arbor_denoiser_infer(arbor_denoiser* d, const uint16_t* features, const float* base, float* denoised, int width, int height) {
   if (int s = live(d, "arbor_denoiser_infer")) return s;
   if (features == nullptr || base == nullptr || denoised == nullptr) {

@@ -382,6 +382,11 @@ ARBOR_API int arbor_denoiser_features(const float* Linear, const float* Guide, c
  * pixel); L1 loss in log(1 + radiance).  loss (host, nullable) receives the
  * batch's mean loss before the step, after the step completes. */
 ARBOR_API int arbor_denoiser_train_step(arbor_denoiser* d, const uint16_t* features, const float* base, const float* target, int batch, int width, int height, float lr, float* loss);
+/* The gradient train_step would apply, without applying it: the loss's
+ * gradient with respect to every parameter (count >= param_count floats,
+ * host memory, the get_params layout) and the loss (host, nullable); the
+ * parameters and the Adam state are unchanged. */
+ARBOR_API int arbor_denoiser_gradient(arbor_denoiser* d, const uint16_t* features, const float* base, const float* target, int batch, int width, int height, float* grad, size_t count, float* loss);
 /* Denoised Linear (float4 per pixel, .w = 1) of one image:
  * exp(log(1 + base) + network) - 1. */
 ARBOR_API int arbor_denoiser_infer(arbor_denoiser* d, const uint16_t* features, const float* base, float* denoised, int width, int height);
