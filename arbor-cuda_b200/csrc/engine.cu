@@ -322,7 +322,7 @@ extern "C" int arbor_engine_inspect(arbor_engine* e, arbor_engine_info* info) {
   info->frames = e->frames;
   info->scene_bytes = e->scene_bytes;
   info->allocated_bytes = e->scene_bytes + kC + kI + arbor_sort_scratch_bytes() + e->image_bytes_total;
-  info->launches_per_frame = 5;  // updateCamera, trace, shadow pass + compose (shadePixels), filterResolve
+  info->launches_per_frame = 6;  // updateCamera, trace, shadow setup + shadow pass + compose (shadePixels), filterResolve
   info->ms_build = e->ms_build;
   info->ms_visibility = e->ms_vis;
   info->ms_lighting = e->ms_light;

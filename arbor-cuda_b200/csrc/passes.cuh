@@ -390,6 +390,74 @@ __device__ __forceinline__ void shadow_pool(const TraceCtx& c, const Camera& cam
   batch_run_pool(c, r, b, policy, pool);
 }
 
+// The same shadow segments with each pixel's ray staged in memory by the
+// setup pass (shadow_setup_px): origin in Vis (w = 1 when the pixel has a
+// shadow ray), direction in Dir.  The tracer's loop then holds no camera or
+// sun-sampling code.
+struct StagedShadowPolicy {
+  static constexpr int kRefill = 8;
+  const TraceCtx* ctx;
+  const float* Dir;
+  float* Vis;
+  int width, height;
+  int pixel, seg;
+  f3 trans, origin, light;
+  __device__ __forceinline__ void start(const TraceCtx& c, Ray& r, int x, int y) {
+    pixel = y * width + x;
+    const float4 o = reinterpret_cast<const float4*>(Vis)[pixel];
+    if (o.w == 1.0f) {
+      origin = mk(o.x, o.y, o.z);
+      light = xyz(__ldg(reinterpret_cast<const float4*>(Dir) + pixel));
+      trans = mk(1.0f, 1.0f, 1.0f);
+      seg = 0;
+      ray_begin(c, r, origin, light, 36.0f);
+    } else {
+      r.phase = kPhIdle;
+    }
+  }
+  __device__ __forceinline__ void write(f3 v) { reinterpret_cast<float4*>(Vis)[pixel] = make_float4(v.x, v.y, v.z, 1.0f); }
+  __device__ __forceinline__ void done(Ray& r) {
+    int id = (int)r.found;
+    if (id < 0) {
+      write(trans);
+    } else if (ldg4(ctx->P, id * 6).w != 1.0f) {
+      write(mk(0.0f, 0.0f, 0.0f));
+    } else {
+      trans = trans * mk(0.18f, 0.29f, 0.065f);
+      origin = origin + light * (r.best + 0.0018f);
+      if (++seg < 4) {
+        ray_begin(*ctx, r, origin, light, 36.0f);
+        return;
+      }
+      write(trans);
+    }
+    r.phase = kPhIdle;
+  }
+};
+
+// Stage pixel (x, y)'s shadow ray for StagedShadowPolicy: origin and w = 1
+// into Vis and the direction into Dir, or Vis.w = 0 without a shadow ray.
+__device__ __forceinline__ void shadow_setup_px(const Camera& cam, const float* __restrict__ Hit, float* __restrict__ Vis, float* __restrict__ Dir,
+                                                int x, int y, int width, int height) {
+  const int pixel = y * width + x;
+  f3 origin, light;
+  if (shadow_ray(cam, __ldg(reinterpret_cast<const float4*>(Hit) + pixel), x, y, width, height, origin, light)) {
+    reinterpret_cast<float4*>(Vis)[pixel] = make_float4(origin.x, origin.y, origin.z, 1.0f);
+    reinterpret_cast<float4*>(Dir)[pixel] = make_float4(light.x, light.y, light.z, 0.0f);
+  } else {
+    reinterpret_cast<float4*>(Vis)[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+}
+
+// Staged shadow segments of every pixel of a persistent CTA's pool.
+template <class WB>
+__device__ __forceinline__ void staged_shadow_pool(const TraceCtx& c, WB& b, const float* __restrict__ Dir, float* __restrict__ Vis,
+                                                   const PixelPool& pool) {
+  StagedShadowPolicy policy{&c, Dir, Vis, pool.width, pool.height, 0, 0};
+  Ray r;
+  batch_run_pool(c, r, b, policy, pool);
+}
+
 // shadePixels' colour of pixel (x, y) (Arbor.cu:277-289), its visibility
 // read from Linear where the shadow pass traced one.
 template <bool kForestScene>

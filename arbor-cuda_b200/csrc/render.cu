@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kBlock, 2) trace_pool_kernel(const float* __re
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock, 2) shadow_pool_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                                 const uint32_t* __restrict__ Order, const float* __restrict__ C,
-                                                                const float* __restrict__ Hit, float* __restrict__ Linear, int width, int height) {
+                                                                const float* __restrict__ Guide, float* __restrict__ Linear, int width, int height) {
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
   __shared__ Camera cam;
@@ -55,7 +55,20 @@ __global__ void __launch_bounds__(kBlock, 2) shadow_pool_kernel(const float* __r
   const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
   const int bx = (width + 7) / 8;
   const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
-  shadow_pool(c, cam, b, Hit, Linear, pool);
+  staged_shadow_pool(c, b, Guide, Linear, pool);
+}
+
+// Stages each pixel's shadow ray for the shadow pass (origin into Linear,
+// direction into Guide; both are overwritten by the compose pass); with sun
+// shadows off it returns at once.
+__global__ void __launch_bounds__(kBlock) shadow_setup_kernel(const float* __restrict__ C, const float* __restrict__ Hit, float* __restrict__ Linear,
+                                                              float* __restrict__ Guide, int width, int height) {
+  __shared__ Camera cam;
+  block_setup(C, cam, nullptr, false);
+  if (!(cam.shadows > 0.5f)) return;
+  int x, y;
+  tile_pixel_at(threadIdx.x, blockIdx.x * kTile, blockIdx.y * kTile, kTile, x, y);
+  if (x < width && y < height) shadow_setup_px(cam, Hit, Linear, Guide, x, y, width, height);
 }
 
 // The compose pass: one pixel per thread, the surface terms and the colour
@@ -238,14 +251,15 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
   }
   // Shadow segments in a persistent pass whose loop holds only the tracer
   // (its code stays small), then the shading of every pixel.
+  shadow_setup_kernel<<<pixel_grid(width, height), kBlock, 0, stream>>>(C, Hit, Linear, Guide, width, height);
   if (forest) {
-    shadow_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, width, height);
+    shadow_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Guide, Linear, width, height);
     shade_compose_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, Normal, width, height);
   } else {
-    shadow_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, Linear, width, height);
+    shadow_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Guide, Linear, width, height);
     shade_compose_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, Normal, width, height);
   }
-  count_launch(2);
+  count_launch(3);
   return check_launch(name);
 }
 

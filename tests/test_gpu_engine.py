@@ -46,7 +46,7 @@ def test_frame_contract(engine):
     n0 = ab.launches()
     engine.frame(1 / 60)
     torch.cuda.synchronize()
-    assert ab.launches() - n0 == engine.inspect().launches_per_frame == 5
+    assert ab.launches() - n0 == engine.inspect().launches_per_frame == 6
     engine.set_input([0] * 32)
     engine.frame(1 / 60)
     px = np.empty(512 * 320, np.uint32)
