@@ -33,6 +33,17 @@ def rnd(n: int, seed: int) -> float:
     return float(np.float32(h & 16777215) / np.float32(16777216.0))
 
 
+def forest_seed(tree: int, ws: int) -> int:
+    """forestSeed (Arbor.cu:57): the per-tree seed of instance `tree` of world seed ws."""
+    return hash_u((tree * 92821 + ws * 68917 + 17) & 0xFFFFFFFF) & 1048575
+
+
+def species_of(n_species: int, ws: int = FOREST_SEED) -> np.ndarray:
+    """Species of each of the 324 instances in a forest of n_species species:
+    forestSeed(t, ws) mod n_species (a seeded, roughly even split)."""
+    return np.array([forest_seed(t, ws) % n_species for t in range(324)], np.int32)
+
+
 def base_state(seed: int, width: int, height: int) -> np.ndarray:
     """initCamera's defaults (Arbor.cu:181) without the pose."""
     C = np.zeros(64, np.float32)

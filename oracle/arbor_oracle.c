@@ -579,11 +579,26 @@ static v3 object_normal(const float* P, int id, v3 p, real fp, real time, real w
   v3 q = vsub(p, ld3(P, b)), h = ld3(P, b + 4);
   return unit(V(q.x / (h.x * h.x), q.y / (h.y * h.y), q.z / (h.z * h.z)));
 }
+/* A forest of several species (no reference counterpart; the reference keeps
+ * one resident tree for all 324 instances, README.md:8): instance t keeps the
+ * reference's transform, phase and tint (forestPos/Scale/Yaw/Seed of t) but
+ * takes its geometry from scene of[t] of the set.  NULL = the reference's
+ * forest, every instance on the one resident scene. */
+typedef struct {
+  const float* const* P;
+  const float* const* N;
+  const uint32_t* const* Order;
+  const int* of;  /* K_FOREST species indices */
+} species_set;
+#define SP_P(sp, tree, base) ((sp) ? (sp)->P[(sp)->of[tree]] : (base))
+#define SP_N(sp, tree, base) ((sp) ? (sp)->N[(sp)->of[tree]] : (base))
+#define SP_O(sp, tree, base) ((sp) ? (sp)->Order[(sp)->of[tree]] : (base))
+
 /* Forest 2D DDA with per-tree bounding spheres (Arbor.cu:235-251).  The
  * single-tree mode (no forest counterpart in the reference) traces the
  * resident tree with an identity instance, as the harness's BVH check does at
  * tests/native_harness.cpp:84. */
-static v2 walk_forest(const float* P, const float* N, const uint32_t* Order, v3 ro, v3 rd, real cone, real time, real wind, real best, int ws, int* tree_out, int shadows) {
+static v2 walk_forest(const float* P, const float* N, const uint32_t* Order, v3 ro, v3 rd, real cone, real time, real wind, real best, int ws, int* tree_out, int shadows, const species_set* sp) {
   int found_tree = -1; real found = -1.0f;
   real half = (real)K_SIDE * K_SPACING * 0.5f;
   v2 world = box_span(ro, rd, V(-half, -1.2f, -half), V(half, 13.5f, half));
@@ -608,7 +623,7 @@ static v2 walk_forest(const float* P, const float* N, const uint32_t* Order, v3 
     if (broad < best) {
       v3 lr = to_local_point(ro, tree, ws), ld = to_local_dir(rd, tree, ws);
       real phase = (real)(tree_seed(tree, ws) & 8191) * 0.0017f;
-      v2 h = walk_tree(P, N, lr, ld, cone / sc, time + phase, wind, best / sc, -1, shadows, Order);
+      v2 h = walk_tree(SP_P(sp, tree, P), SP_N(sp, tree, N), lr, ld, cone / sc, time + phase, wind, best / sc, -1, shadows, SP_O(sp, tree, Order));
       if (h.y >= 0.0f && h.x * sc < best) { best = h.x * sc; found = h.y; found_tree = tree; }
     }
     real next = tx < tz ? tx : tz;
@@ -618,18 +633,18 @@ static v2 walk_forest(const float* P, const float* N, const uint32_t* Order, v3 
   *tree_out = found_tree;
   return V2(best, found);
 }
-static v2 walk_scene(const float* P, const float* N, const uint32_t* Order, v3 ro, v3 rd, real cone, real time, real wind, real best, int ws, int* tree_out, int shadows, int single) {
-  if (!single) return walk_forest(P, N, Order, ro, rd, cone, time, wind, best, ws, tree_out, shadows);
+static v2 walk_scene(const float* P, const float* N, const uint32_t* Order, v3 ro, v3 rd, real cone, real time, real wind, real best, int ws, int* tree_out, int shadows, int single, const species_set* sp) {
+  if (!single) return walk_forest(P, N, Order, ro, rd, cone, time, wind, best, ws, tree_out, shadows, sp);
   *tree_out = -1;
   return walk_tree(P, N, ro, rd, cone, time, wind, best, -1, shadows, Order);
 }
 /* One pixel of tracePixels (Arbor.cu:252). */
-static void trace_px(const float* P, const float* N, const uint32_t* Order, const float* C, float* Hit, int w, int h, int x, int y, int single) {
+static void trace_px(const float* P, const float* N, const uint32_t* Order, const float* C, float* Hit, int w, int h, int x, int y, int single, const species_set* sp) {
   int b = (y * w + x) * 4;
   v3 ro = cam_pos(C), rd = primary_dir(C, x, y, w, h);
   real ground = rd.y < -0.00001f ? -ro.y / rd.y : K_FAR;
   int tree = -1;
-  v2 r = walk_scene(P, N, Order, ro, rd, C[14] / (real)h, C[8], C[11], ground > 0.0f ? ground : K_FAR, (int)C[31], &tree, 0, single);
+  v2 r = walk_scene(P, N, Order, ro, rd, C[14] / (real)h, C[8], C[11], ground > 0.0f ? ground : K_FAR, (int)C[31], &tree, 0, single, sp);
   Hit[b] = (float)r.x; Hit[b + 1] = (float)r.y; Hit[b + 2] = (float)tree; Hit[b + 3] = (float)(C[14] * r.x / (real)h);
 }
 
@@ -713,14 +728,14 @@ static v3 albedo_of(const float* P, int id, v3 p, real fp, real time, real wind)
   return mixv(V(0.09f, 0.10f, 0.086f), V(0.31f, 0.30f, 0.24f), f);
 }
 /* Sun visibility through at most four segments (Arbor.cu:271-274). */
-static v3 sun_visibility(const float* P, const float* N, const uint32_t* Order, v3 p, v3 dir, real time, real wind, int ws, int single) {
+static v3 sun_visibility(const float* P, const float* N, const uint32_t* Order, v3 p, v3 dir, real time, real wind, int ws, int single, const species_set* sp) {
   v3 trans = V(1.0f, 1.0f, 1.0f); v3 ro = p;
   for (int j = 0; j < 4; j++) {
     int tree = -1;
-    v2 h = walk_scene(P, N, Order, ro, dir, 0.0001f, time, wind, 36.0f, ws, &tree, 1, single);
+    v2 h = walk_scene(P, N, Order, ro, dir, 0.0001f, time, wind, 36.0f, ws, &tree, 1, single, sp);
     int id = (int)h.y;
     if (id < 0) break;
-    if (P[id * K_PS + 3] != 1.0f) return V(0.0f, 0.0f, 0.0f);
+    if (SP_P(sp, tree, P)[id * K_PS + 3] != 1.0f) return V(0.0f, 0.0f, 0.0f);
     trans = vmul(trans, V(0.18f, 0.29f, 0.065f));
     ro = vadd(ro, vscale(dir, h.x + 0.0018f));
   }
@@ -738,34 +753,51 @@ static real ggx(v3 n, v3 v, v3 l, real rough) {
   real F = 0.035f + 0.965f * POW(1.0f - vh, 5.0f);
   return D * G * F / (4.0f * nv + 0.0001f);
 }
+/* The surface point of a hit pixel and its shading normal, facing the
+ * camera (Arbor.cu:278-280: the first steps of shadePixels). */
+typedef struct { v3 p, lp, n; real fp, lfp, phase; int leaf; } surface;
+static surface shade_surface(const float* P, const float* C, const float* Hit, v3 ro, v3 rd, int b, int single) {
+  surface s;
+  real t = Hit[b]; int id = (int)Hit[b + 1], tree = (int)Hit[b + 2];
+  int ws = (int)C[31];
+  v3 p = vadd(ro, vscale(rd, t));
+  real fp = FMAX(0.000005f, Hit[b + 3]);
+  v3 lp = p, n = V(0.0f, 1.0f, 0.0f);
+  real lfp = fp, phase = 0.0f;
+  if (id >= 0 && tree >= 0) {
+    real sc = tree_scale(tree, ws);
+    lp = to_local_point(p, tree, ws); lfp = fp / sc;
+    phase = (real)(tree_seed(tree, ws) & 8191) * 0.0017f;
+    n = to_world_normal(object_normal(P, id, lp, lfp, C[8] + phase, C[11]), tree, ws);
+  } else if (id >= 0 && single) {
+    n = object_normal(P, id, lp, lfp, C[8], C[11]);
+  }
+  s.leaf = id >= 0 && P[id * K_PS + 3] == 1.0f;
+  if (dot(n, rd) > 0.0f) n = vscale(n, -1.0f);
+  if (id < 0) {
+    real e = FMAX(0.001f, fp);
+    real nx = (noise2((p.x + e) * 18.0f, p.z * 18.0f, 133) - noise2((p.x - e) * 18.0f, p.z * 18.0f, 133)) * 0.18f;
+    real nz = (noise2(p.x * 18.0f, (p.z + e) * 18.0f, 133) - noise2(p.x * 18.0f, (p.z - e) * 18.0f, 133)) * 0.18f;
+    n = unit(V(nx, 1.0f, nz));
+  }
+  s.p = p; s.lp = lp; s.n = n; s.fp = fp; s.lfp = lfp; s.phase = phase;
+  return s;
+}
 /* One pixel of shadePixels (Arbor.cu:277-289). */
-static void shade_px(const float* P, const float* N, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int w, int hgt, int x, int y, int single) {
+static void shade_px(const float* Pw, const float* N, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int w, int hgt, int x, int y, int single, const species_set* sp) {
   int pixel = y * w + x, b = pixel * 4;
   real t = Hit[b]; int id = (int)Hit[b + 1], tree = (int)Hit[b + 2];
   v3 ro = cam_pos(C), rd = primary_dir(C, x, y, w, hgt), sun = sun_dir(C);
   v3 col = sky(rd, sun), guide = V(1.0f, 1.0f, 1.0f);
   int ws = (int)C[31];
+  /* the hit instance's scene (its species' scene in a forest of several) */
+  const float* P = (tree >= 0 && tree < K_SIDE * K_SIDE) ? SP_P(sp, tree, Pw) : Pw;
   if (t < K_FAR) {
-    v3 p = vadd(ro, vscale(rd, t));
-    real fp = FMAX(0.000005f, Hit[b + 3]);
-    v3 lp = p, n = V(0.0f, 1.0f, 0.0f);
-    real lfp = fp, phase = 0.0f;
-    if (id >= 0 && tree >= 0) {
-      real sc = tree_scale(tree, ws);
-      lp = to_local_point(p, tree, ws); lfp = fp / sc;
-      phase = (real)(tree_seed(tree, ws) & 8191) * 0.0017f;
-      n = to_world_normal(object_normal(P, id, lp, lfp, C[8] + phase, C[11]), tree, ws);
-    } else if (id >= 0 && single) {
-      n = object_normal(P, id, lp, lfp, C[8], C[11]);
-    }
-    int leaf = id >= 0 && P[id * K_PS + 3] == 1.0f;
-    if (dot(n, rd) > 0.0f) n = vscale(n, -1.0f);
-    if (id < 0) {
-      real e = FMAX(0.001f, fp);
-      real nx = (noise2((p.x + e) * 18.0f, p.z * 18.0f, 133) - noise2((p.x - e) * 18.0f, p.z * 18.0f, 133)) * 0.18f;
-      real nz = (noise2(p.x * 18.0f, (p.z + e) * 18.0f, 133) - noise2(p.x * 18.0f, (p.z - e) * 18.0f, 133)) * 0.18f;
-      n = unit(V(nx, 1.0f, nz));
-    }
+    surface s = shade_surface(P, C, Hit, ro, rd, b, single);
+    v3 p = s.p, lp = s.lp, n = s.n;
+    real fp = s.fp, lfp = s.lfp, phase = s.phase;
+    int leaf = s.leaf;
+    (void)fp;
     v3 albedo = albedo_of(P, id, id >= 0 ? lp : p, lfp, C[8] + phase, C[11]);
     if (tree >= 0) {
       int ts = tree_seed(tree, ws);
@@ -784,7 +816,7 @@ static void shade_px(const float* P, const float* N, const uint32_t* Order, cons
     v3 light = unit(vadd(vadd(sun, vscale(su, COS(angle) * disk)), vscale(sv, SIN(angle) * disk)));
     real offset = id >= 0 ? 0.0014f : 0.004f;
     v3 vis = V(1.0f, 1.0f, 1.0f);
-    if (C[22] > 0.5f) vis = sun_visibility(P, N, Order, vadd(p, vscale(light, offset)), light, C[8], C[11], ws, single);
+    if (C[22] > 0.5f) vis = sun_visibility(Pw, N, Order, vadd(p, vscale(light, offset)), light, C[8], C[11], ws, single, sp);
     real nl = sat(dot(n, light)), back = sat(-dot(n, light));
     v3 direct = vscale(albedo, nl / K_PI);
     if (leaf) {
@@ -975,12 +1007,46 @@ EXPORT void oracle_updateCamera(float* C, const float* I, const float* P, float 
 EXPORT void oracle_tracePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int w, int h, int y0, int y1, int single) {
 #pragma omp parallel for schedule(dynamic, 2)
   for (int y = y0; y < y1; y++)
-    for (int x = 0; x < w; x++) trace_px(P, Nodes, Order, C, Hit, w, h, x, y, single);
+    for (int x = 0; x < w; x++) trace_px(P, Nodes, Order, C, Hit, w, h, x, y, single, NULL);
 }
 EXPORT void oracle_shadePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int w, int h, int y0, int y1, int single) {
 #pragma omp parallel for schedule(dynamic, 2)
   for (int y = y0; y < y1; y++)
-    for (int x = 0; x < w; x++) shade_px(P, Nodes, Order, C, Hit, Linear, Guide, w, h, x, y, single);
+    for (int x = 0; x < w; x++) shade_px(P, Nodes, Order, C, Hit, Linear, Guide, w, h, x, y, single, NULL);
+}
+/* tracePixels / shadePixels over a forest of several species: instance t
+ * takes its geometry from scene of[t] (P[of[t]], Nodes[of[t]],
+ * Order[of[t]]), everything else as in the reference's forest (rows
+ * y0..y1-1).  No reference counterpart: the reference's instances all share
+ * one resident tree (README.md:8, docs/ARCHITECTURE.md:5); with every of[t]
+ * equal this is its tracePixels / shadePixels. */
+EXPORT void oracle_tracePixelsSpecies(const float* const* P, const float* const* N, const uint32_t* const* Order, const int* of, const float* C,
+                                      float* Hit, int w, int h, int y0, int y1) {
+  species_set sp = {P, N, Order, of};
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int y = y0; y < y1; y++)
+    for (int x = 0; x < w; x++) trace_px(P[0], N[0], Order[0], C, Hit, w, h, x, y, 0, &sp);
+}
+EXPORT void oracle_shadePixelsSpecies(const float* const* P, const float* const* N, const uint32_t* const* Order, const int* of, const float* C,
+                                      const float* Hit, float* Linear, float* Guide, int w, int h, int y0, int y1) {
+  species_set sp = {P, N, Order, of};
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int y = y0; y < y1; y++)
+    for (int x = 0; x < w; x++) shade_px(P[0], N[0], Order[0], C, Hit, Linear, Guide, w, h, x, y, 0, &sp);
+}
+/* The shading normal shadePixels computes for each pixel (world space,
+ * facing the camera), zero for sky pixels: rows y0..y1-1 of Normal (w*h
+ * float4, .w = 0).  The reference keeps this value inside shadePixels; its
+ * view mode 3 writes it as n * 0.5 + 0.5 (Arbor.cu:286). */
+EXPORT void oracle_shadeNormals(const float* P, const float* C, const float* Hit, float* Normal, int w, int h, int y0, int y1, int single) {
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int y = y0; y < y1; y++)
+    for (int x = 0; x < w; x++) {
+      int b = (y * w + x) * 4;
+      v3 n = V(0.0f, 0.0f, 0.0f);
+      if (Hit[b] < K_FAR) n = shade_surface(P, C, Hit, cam_pos(C), primary_dir(C, x, y, w, h), b, single).n;
+      st3(Normal, b, n); Normal[b + 3] = 0.0f;
+    }
 }
 EXPORT void oracle_filterLighting(const float* Linear, const float* Guide, const float* Hit, float* Filtered, const float* C, int w, int h, int y0, int y1) {
 #pragma omp parallel for schedule(dynamic, 2)
@@ -996,7 +1062,7 @@ EXPORT void oracle_resolvePixels(const float* Filtered, float* History, uint32_t
  * mismatching pixels). */
 EXPORT void oracle_tracePixelList(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int w, int h, const int* xy, int n, int single) {
 #pragma omp parallel for schedule(dynamic, 4)
-  for (int i = 0; i < n; i++) trace_px(P, Nodes, Order, C, Hit, w, h, xy[2 * i], xy[2 * i + 1], single);
+  for (int i = 0; i < n; i++) trace_px(P, Nodes, Order, C, Hit, w, h, xy[2 * i], xy[2 * i + 1], single, NULL);
 }
 /* Function-level probes (the harness's checks at tests/native_harness.cpp:84-92). */
 EXPORT void oracle_traceTreeRay(const float* P, const float* Nodes, const uint32_t* Order, const float* ro, const float* rd, float cone, float time, float wind, float best, int ignore, int shadows, float* out) {
@@ -1080,10 +1146,10 @@ EXPORT void oracle_frameRows(const float* P, const float* Nodes, const uint32_t*
                              float* Filtered, float* History, uint32_t* Pixels, int w, int h, const int* rows, int n, int single) {
 #pragma omp parallel for schedule(dynamic, 2)
   for (int i = 0; i < n; i++)
-    for (int x = 0; x < w; x++) trace_px(P, Nodes, Order, C, Hit, w, h, x, rows[i], single);
+    for (int x = 0; x < w; x++) trace_px(P, Nodes, Order, C, Hit, w, h, x, rows[i], single, NULL);
 #pragma omp parallel for schedule(dynamic, 2)
   for (int i = 0; i < n; i++)
-    for (int x = 0; x < w; x++) shade_px(P, Nodes, Order, C, Hit, Linear, Guide, w, h, x, rows[i], single);
+    for (int x = 0; x < w; x++) shade_px(P, Nodes, Order, C, Hit, Linear, Guide, w, h, x, rows[i], single, NULL);
 #pragma omp parallel for schedule(dynamic, 2)
   for (int i = 0; i < n; i++)
     for (int x = 0; x < w; x++) filter_px(Linear, Guide, Hit, Filtered, C, w, h, x, rows[i]);

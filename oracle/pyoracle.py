@@ -17,7 +17,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_DIR = os.environ.get("ARBOR_REFERENCE_DIR", "/root/reference")
+# The reference checkout: $ARBOR_REFERENCE_DIR, else a directory named
+# "reference" beside this repository's root.
+REFERENCE_DIR = os.environ.get("ARBOR_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 
 CAPACITY = 32768
 NODE_COUNT = 65536
@@ -73,6 +75,12 @@ _SIGNATURES = {
 _OPTIONAL = {
     # only in the reference build: the harness's Renderer constructor
     "oracle_harnessBuild": (None, [_c_int, _f, _f, _u, _u, _f]),
+    # only in the port: shadePixels' shading normal per pixel, and the forest
+    # of several species (no reference counterpart)
+    "oracle_shadeNormals": (None, [_f, _f, _f, _f, _c_int, _c_int, _c_int, _c_int, _c_int]),
+    "oracle_tracePixelsSpecies": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i, _f, _f, _c_int, _c_int, _c_int, _c_int]),
+    "oracle_shadePixelsSpecies": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i, _f, _f, _f, _f, _c_int, _c_int, _c_int,
+                                         _c_int]),
 }
 
 
@@ -220,6 +228,38 @@ class Oracle:
         Linear = np.zeros(w * h * 4, np.float32) if Linear is None else Linear
         Guide = np.zeros(w * h * 4, np.float32) if Guide is None else Guide
         self.lib.oracle_shadePixels(_p(scene["P"]), _p(scene["Nodes"]), _p(scene["Order"]), _p(C), _p(Hit), _p(Linear), _p(Guide), w, h, y0, y1, int(single))
+        return Linear, Guide
+
+    def shade_normals(self, scene, C, Hit, w, h, y0=0, y1=None, single=False, Normal=None):
+        """shadePixels' shading normal per pixel (world space, facing the camera; zero for sky)."""
+        y1 = h if y1 is None else y1
+        Normal = np.zeros(w * h * 4, np.float32) if Normal is None else Normal
+        self.lib.oracle_shadeNormals(_p(scene["P"]), _p(C), _p(Hit), _p(Normal), w, h, y0, y1, int(single))
+        return Normal
+
+    @staticmethod
+    def _species_tables(scenes: list, of):
+        keep = [np.ascontiguousarray(s[k]) for s in scenes for k in ("P", "Nodes", "Order")]
+        ptr = lambda key: (ctypes.c_void_p * len(scenes))(*[s[key].ctypes.data for s in scenes])  # noqa: E731
+        of = np.ascontiguousarray(of, dtype=np.int32)
+        assert of.shape == (324,) and of.min() >= 0 and of.max() < len(scenes)
+        return ptr("P"), ptr("Nodes"), ptr("Order"), of, keep
+
+    def trace_species(self, scenes: list, of, C, w, h, y0=0, y1=None, Hit=None):
+        """tracePixels over a forest whose instance t uses scenes[of[t]]."""
+        y1 = h if y1 is None else y1
+        Hit = np.zeros(w * h * 4, np.float32) if Hit is None else Hit
+        P, N, O, of, _keep = self._species_tables(scenes, of)
+        self.lib.oracle_tracePixelsSpecies(P, N, O, _p(of), _p(C), _p(Hit), w, h, y0, y1)
+        return Hit
+
+    def shade_species(self, scenes: list, of, C, Hit, w, h, y0=0, y1=None, Linear=None, Guide=None):
+        """shadePixels over a forest whose instance t uses scenes[of[t]]."""
+        y1 = h if y1 is None else y1
+        Linear = np.zeros(w * h * 4, np.float32) if Linear is None else Linear
+        Guide = np.zeros(w * h * 4, np.float32) if Guide is None else Guide
+        P, N, O, of, _keep = self._species_tables(scenes, of)
+        self.lib.oracle_shadePixelsSpecies(P, N, O, _p(of), _p(C), _p(Hit), _p(Linear), _p(Guide), w, h, y0, y1)
         return Linear, Guide
 
     def filter(self, Linear, Guide, Hit, C, w, h, y0=0, y1=None, Filtered=None):

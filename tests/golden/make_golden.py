@@ -107,6 +107,14 @@ def main() -> None:
         ref.update_camera(Cw, I, sc7["P"], dt, 192, 108)
         walk.append(Cw.tolist())
     gold["walk_seed7_C"] = walk
+    # The measured walk: camera record after each of the 64 frames at 1920x1080.
+    walk = []
+    Cw = ref.init_camera(sc7["P"], 7)
+    for frame in range(64):
+        I, dt = workloads.walk_input(frame)
+        ref.update_camera(Cw, I, sc7["P"], dt, 1920, 1080)
+        walk.append(Cw.tolist())
+    gold["walk_seed7_1080p_C"] = walk
 
     # The harness's recorded check values.
     rays = harness_rays(ref, scene)

@@ -209,3 +209,55 @@ def test_f64_rerun_close_to_f32(oracle, oracle64, scenes):
     both = same & (h32[:, 0] < 1e5)
     rel = np.abs(h32[both, 0] - h64[both, 0]) / h64[both, 0]
     assert np.median(rel) < 1e-5 and np.quantile(rel, 0.99) < 2e-3
+
+
+@pytest.mark.parametrize("view", [1, 2, 5])
+def test_shade_normals_are_the_view_mode_3_normals(oracle, scenes, view):
+    """oracle_shadeNormals gives the normal shadePixels computes: the
+    reference's view mode 3 writes it as n * 0.5 + 0.5 (Arbor.cu:286), and
+    the mode-3 frame of the oracle is pinned to the reference's digest."""
+    w, h = 96, 64
+    s = scenes(1788)
+    C = np.array(GOLD["frames_1788_96x64"][f"view{view}_light0_mode0"]["C"], np.float32)
+    C[15] = 3.0
+    hit = oracle.trace(s, C, w, h)
+    lin, _ = oracle.shade(s, C, hit, w, h)
+    n = oracle.shade_normals(s, C, hit, w, h).reshape(-1, 4)
+    surf = hit.reshape(-1, 4)[:, 0] < 1e5
+    decoded = (lin.reshape(-1, 4)[:, :3] - 0.5) * 2.0
+    assert surf.any()
+    assert np.abs(n[surf, :3] - decoded[surf]).max() <= 2.5e-7
+    assert (n[~surf] == 0).all() and (n[:, 3] == 0).all()
+    near = hit.reshape(-1, 4)[:, 0] < 1000.0  # far hits have footprints wider than the primitive: degenerate normals
+    assert np.allclose(np.linalg.norm(n[near, :3], axis=1), 1.0, atol=1e-5)
+
+
+def test_walk_1080p_camera_records(oracle, scenes):
+    """The measured walk's 64 camera records at 1920x1080 equal the reference's."""
+    import workloads
+
+    P = scenes(7)["P"]
+    C = oracle.init_camera(P, 7)
+    for frame, want in enumerate(GOLD["walk_seed7_1080p_C"]):
+        I, dt = workloads.walk_input(frame)
+        oracle.update_camera(C, I, P, dt, 1920, 1080)
+        assert np.array_equal(u32(C), u32(np.array(want, np.float32))), f"frame {frame}"
+
+
+def test_species_forest_with_one_species_is_the_forest(oracle, scenes):
+    """The forest of several species with every instance on scene 0 renders
+    exactly the reference's forest (oracle_tracePixelsSpecies /
+    oracle_shadePixelsSpecies against the forest passes)."""
+    import workloads
+
+    s = scenes(7)
+    C = oracle.init_camera(s["P"], 7)
+    C[32], C[33], C[22] = 160, 96, 1.0
+    want = oracle.frame(s, C, 160, 96)
+    hit = oracle.trace_species([s], np.zeros(324, np.int32), C, 160, 96)
+    lin, gui = oracle.shade_species([s], np.zeros(324, np.int32), C, hit, 160, 96)
+    assert np.array_equal(u32(hit), u32(want["Hit"]))
+    assert np.array_equal(u32(lin), u32(want["Linear"])) and np.array_equal(u32(gui), u32(want["Guide"]))
+    of = workloads.species_of(3, 7)
+    assert sorted(set(of.tolist())) == [0, 1, 2]
+    assert [workloads.forest_seed(t, 7) for t in range(324)] == GOLD["forest_seeds_seed7"]
