@@ -634,11 +634,14 @@ __global__ void __launch_bounds__(kSortThreads) radix_pass_n_kernel(const uint32
   }
 }
 
-// Device address of the scratch array, looked up once per device.
+// Device address of the scratch array on each device.  A call outside stream
+// capture looks it up again (a device reset reloads the library's module,
+// and the array may then sit elsewhere); a call during capture uses the
+// address its device's last call outside capture found.
 std::mutex g_noalloc_mutex;
 uint32_t* g_noalloc_ptr[64] = {};
 
-int noalloc_scratch(uint32_t** out) {
+int noalloc_scratch(cudaStream_t stream, uint32_t** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) {
@@ -649,8 +652,13 @@ int noalloc_scratch(uint32_t** out) {
     set_error("arbor_sortKeysNoAlloc: device %d is beyond the 64 devices this library tracks", dev);
     return ARBOR_ERR_LIMIT;
   }
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess) {
+    (void)cudaGetLastError();  // the query's own error; treat the stream as capturing
+    capture = cudaStreamCaptureStatusActive;
+  }
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_ptr[dev] == nullptr) {
+  if (g_noalloc_ptr[dev] == nullptr || capture == cudaStreamCaptureStatusNone) {
     void* ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_noalloc_sort_scratch);
     if (e != cudaSuccess || ptr == nullptr) {
@@ -680,7 +688,7 @@ extern "C" int arbor_sortKeysNoAlloc(uint32_t* Keys, uint32_t* Order, int count,
   if (int s = check_bindings(name, b)) return s;
   if (count == 0) return ARBOR_OK;
   uint32_t* scratch = nullptr;
-  if (int s = noalloc_scratch(&scratch)) return s;
+  if (int s = noalloc_scratch(stream, &scratch)) return s;
   uint32_t* k2 = scratch;
   uint32_t* v2 = scratch + kNoAllocMaxPairs;
   int ctas = (count + kSortPerCta - 1) / kSortPerCta;

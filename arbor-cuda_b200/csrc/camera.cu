@@ -115,10 +115,26 @@ __global__ void set_sample_kernel(float* C, int sample, int reset) {
   C[10] = reset ? 1.0f : 0.0f;
 }
 
+// The forest instance table of world seed ws, one Instance per tree: the
+// table every trace/shade CTA builds in shared memory (render_common.cuh).
+__global__ void forest_instances_kernel(Instance* out, int ws) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < kForest) out[t] = make_instance(t, ws);
+}
+
 }  // namespace
 }  // namespace arbor
 
 using namespace arbor;
+
+extern "C" int arbor_forestInstances(int world_seed, float* instances, arbor_stream stream) {
+  static_assert(sizeof(Instance) == ARBOR_INSTANCE_FLOATS * 4, "Instance record layout");
+  const Binding b[] = {{instances, (size_t)kForest * sizeof(Instance), true, 16, "instances"}};
+  if (int s = check_bindings("arbor_forestInstances", b)) return s;
+  forest_instances_kernel<<<(kForest + 127) / 128, 128, 0, stream>>>(reinterpret_cast<Instance*>(instances), world_seed);
+  count_launch();
+  return check_launch("arbor_forestInstances");
+}
 
 extern "C" int arbor_setSample(float* C, int sample, int reset, arbor_stream stream) {
   const Binding b[] = {{C, kC, true, 4, "C"}};

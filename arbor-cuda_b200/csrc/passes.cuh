@@ -324,14 +324,21 @@ __device__ __forceinline__ f3 shade_post(const Shading& o, f3 visibility) {
   return mix3(col, o.skyc, o.haze);
 }
 
-// The shadow ray of pixel (x, y), when shadePixels traces one: a surface hit
-// (not sky), no debug view, sun shadows on.  The same values shade_pre
-// computes for the pixel.
+// Whether shadePixels traces a shadow ray for a pixel whose hit distance is
+// t: a surface hit (not sky), no debug view, sun shadows on (Arbor.cu:283,
+// 286).  The shadow setup pass stages a ray exactly where this holds, and the
+// compose pass reads the shadow pass's visibility exactly where it holds.
+__device__ __forceinline__ bool traces_shadow(const Camera& cam, float t) {
+  return t < kFar && !(cam.mode == 1.0f || cam.mode == 2.0f || cam.mode == 3.0f) && cam.shadows > 0.5f;
+}
+
+// The shadow ray of pixel (x, y), when shadePixels traces one.  The same
+// values shade_pre computes for the pixel.
 __device__ __forceinline__ bool shadow_ray(const Camera& cam, float4 hit, int x, int y, int width, int height, f3& origin, f3& light) {
   const float t = hit.x;
   int id = (int)hit.y;
   if (id >= kCapacity) id = -1;
-  if (!(t < kFar) || cam.mode == 1.0f || cam.mode == 2.0f || cam.mode == 3.0f || !(cam.shadows > 0.5f)) return false;
+  if (!traces_shadow(cam, t)) return false;
   const f3 p = cam.ro + camera_ray(cam, x, y, width, height) * t;
   light = sun_sample(cam, y * width + x);
   origin = shadow_origin(p, light, id);
@@ -465,10 +472,11 @@ __device__ __forceinline__ void shade_compose_px(const float* __restrict__ P, co
                                                  float* __restrict__ Linear, float* __restrict__ Guide, float* __restrict__ Normal, int x, int y,
                                                  int width, int height) {
   const int pixel = y * width + x;
+  const float4 hit = __ldg(reinterpret_cast<const float4*>(Hit) + pixel);
   Shading sh;
-  shade_pre<kForestScene>(P, cam, inst, __ldg(reinterpret_cast<const float4*>(Hit) + pixel), x, y, width, height, sh);
+  shade_pre<kForestScene>(P, cam, inst, hit, x, y, width, height, sh);
   f3 vis = mk(1.0f, 1.0f, 1.0f);
-  if (!sh.final && sh.shadow) vis = xyz(reinterpret_cast<const float4*>(Linear)[pixel]);
+  if (traces_shadow(cam, hit.x)) vis = xyz(reinterpret_cast<const float4*>(Linear)[pixel]);
   const f3 col = shade_post(sh, vis);
   reinterpret_cast<float4*>(Linear)[pixel] = make_float4(col.x, col.y, col.z, 1.0f);
   reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);

@@ -1,14 +1,18 @@
 """Benchmark: the 324-tree 1920x1080 forest walk (1 spp, sun shadows off).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl arbor|reference]
-                    [--workload forest|shadows|tree] [--no-cpu-baseline]
+                    [--workload forest|shadows|wind|tree|batch|denoise] [--no-cpu-baseline]
+                    [--no-target]
 
 A step is one frame of the seeded 64-frame walk: updateCamera, tracePixels,
 shadePixels and filterLighting+resolvePixels over 1920x1080 pixels, on a
 scene (master seed 7) built once.  `value` is primary rays per second of the
 whole job (all ranks) with inputs resident on the device; `e2e` is the same
 metric through the engine API with the input record copied from pinned host
-memory and the RGBA8 frame copied back to the host every step.
+memory and the RGBA8 frame copied back to the host every step.  The default
+forest run then measures the same walk with tree-to-tree sun shadows on (the
+target configuration) and reports it, with its own CPU baseline, under
+`target_shadows`.
 
 Multi-GPU: the path shards by frames/pixels with no exchange, so each rank
 renders its own frames (weak scaling, replicas); timing is the max over ranks.
@@ -54,6 +58,8 @@ def parse():
     ap.add_argument("--width", type=int, default=0, help="override the workload's width (profiling runs)")
     ap.add_argument("--height", type=int, default=0, help="override the workload's height (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the engine-API end-to-end leg (profiling runs)")
+    ap.add_argument("--no-target", action="store_true",
+                    help="forest workload: skip the second measurement of the same walk with sun shadows on (target_shadows)")
     return ap.parse_args()
 
 
@@ -260,14 +266,37 @@ def measured_peaks() -> dict:
 
 
 def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
+    spec = workload_spec(args.workload)
+    if args.width and args.height:
+        spec.update(width=args.width, height=args.height, workload=spec["workload"] + f" (at {args.width}x{args.height})")
+    result = measure_workload(args, spec, rank, world, local_rank)
+    if args.workload == "forest" and not args.no_target:
+        # The target configuration: the same walk with tree-to-tree sun
+        # shadows on, measured the same way, with its own CPU baseline.
+        tspec = workload_spec("shadows")
+        if args.width and args.height:
+            tspec.update(width=args.width, height=args.height, workload=tspec["workload"] + f" (at {args.width}x{args.height})")
+        t = measure_workload(args, tspec, rank, world, local_rank)
+        keep = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config", "phases_ms", "roofline", "roofline_trace",
+                "roofline_shade", "roofline_hbm", "gpu_launches", "clocks", "e2e", "cpu_baseline")
+        result["target_shadows"] = {k: t[k] for k in keep if k in t}
+        cpu = t.get("cpu_baseline", {}).get("value")
+        e2e = (t.get("e2e") or {}).get("value")
+        if cpu and e2e:
+            result["target_shadows"]["e2e_over_cpu_baseline"] = round(e2e / cpu, 1)
+        result["gpu_launches"] += t["gpu_launches"]
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def measure_workload(args, spec: dict, rank: int, world: int, local_rank: int) -> dict:
+    """Time `args.steps` frames of one workload (after `args.warmup`) and
+    return its JSON record (every rank calls it; max over ranks)."""
     import torch
     import torch.distributed as dist
 
     import arbor_b200 as ab
 
-    spec = workload_spec(args.workload)
-    if args.width and args.height:
-        spec.update(width=args.width, height=args.height, workload=spec["workload"] + f" (at {args.width}x{args.height})")
     fr = Frames(ab, spec, torch)
     w, h = fr.w, fr.h
     for k in range(args.warmup):
@@ -352,8 +381,8 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
             result["e2e"] = {"value": None, "unit": UNIT, "note": "the engine API renders one sample per frame without rebuilds"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(spec, args.cpu_seconds)
-    if rank == 0:
-        print(json.dumps(result), flush=True)
+    del fr
+    return result
 
 
 def run_e2e(ab, torch, spec: dict, args) -> dict:

@@ -165,9 +165,11 @@ ARBOR_API int arbor_sortKeys(uint32_t* Keys, uint32_t* Order, void* scratch, arb
  * (Keys, Order) pairs, count <= 32768, in the same order arbor_sortKeys
  * gives; a larger count returns ARBOR_ERR_LIMIT.  It allocates nothing: its
  * ping-pong buffer is a fixed 256 KB array inside the library, which every
- * GPU that loads the library keeps until the process exits.  The first call
- * on each device looks up that array's device address (cudaGetSymbolAddress),
- * so make the first call on a device before any stream capture.  All calls
+ * GPU that loads the library keeps until the process exits.  A call outside
+ * stream capture looks up that array's device address (cudaGetSymbolAddress);
+ * a call during capture reuses the address its device's last call outside
+ * capture found, so make one call on a device before capturing, and again
+ * after a device reset (which can move the array).  All calls
  * share the one array: calls that overlap on the GPU (different streams, no
  * ordering between them) race and corrupt each other's results. */
 ARBOR_API int arbor_sortKeysNoAlloc(uint32_t* Keys, uint32_t* Order, int count, arbor_stream stream);
@@ -209,6 +211,17 @@ ARBOR_API int arbor_shadeGBuffer(const float* P, const float* Nodes, const uint3
 /* filterLighting followed by resolvePixels in one launch; writes Filtered,
  * History and Pixels exactly as the two separate entries do. */
 ARBOR_API int arbor_filterResolve(const float* Linear, const float* Guide, const float* Hit, float* Filtered, float* History, uint32_t* Pixels, const float* C, int width, int height, arbor_stream stream);
+
+/* The forest instance table of a world seed (C[31]): per tree t of the
+ * 18x18 grid, the values the reference's forest helpers compute on the fly
+ * (forestSeed, forestPos, forestScale, forestYaw, the wind phase;
+ * Arbor.cu:57-69, 279), as the trace and shade kernels hold them.  Writes
+ * ARBOR_FOREST_COUNT records of ARBOR_INSTANCE_FLOATS 4-byte words:
+ * {pos.x, pos.z, scale, sphere centre y = 4.4 scale, sphere radius = 6.6
+ * scale, cos(-yaw), sin(-yaw), cos(yaw), sin(yaw), phase, seed (int32), 0}.
+ * Inspection helper; no single reference counterpart. */
+#define ARBOR_INSTANCE_FLOATS 12
+ARBOR_API int arbor_forestInstances(int world_seed, float* instances, arbor_stream stream);
 
 /* Profiling helper (no reference counterpart): counts the traversal and
  * intersection events one tracePixels (single_tree = 0) or traceTreePixels

@@ -15,8 +15,9 @@ reference's order.  Where a hit lies before its box's entry (a surface
 reaching outside its box, or the box entry rounding past the hit), the
 reference can prune that box after finding a farther hit, and the batched
 pass, which tested the box before the farther hit came back, keeps the
-nearer one.  The bar: at most 1 pixel in 10^5 differs, and at every
-differing pixel the batched hit is the nearer one.  Checked on full-HD
+nearer one.  The bar: no more differing pixels than measured per case
+(MAX_DIFFERING), and at every differing pixel the batched hit is the nearer
+one.  Checked on full-HD
 frames of the forest walk with sun shadows on and on the single-tree scene.
 """
 import numpy as np
@@ -57,7 +58,12 @@ def render_both(ab, s, w, h, single):
     return (hit, hit_ref), (lin, lin_ref), (gui, gui_ref)
 
 
-MAX_DIFFERING = 1e-5  # fraction of pixels
+# Pixels whose Hit / Linear may differ from the in-order traversal's, per
+# case: the counts measured on the B200 (walk frame 0: two pixels, each a hit
+# the in-order traversal pruned because it lies before its box's entry, and
+# one Linear through a shadow segment; none elsewhere).  Any new difference
+# fails the test.
+MAX_DIFFERING = {"walk frame 0": (2, 1), "walk frame 23": (0, 0), "single tree": (0, 0)}
 
 
 def report(label, pairs, w, h):
@@ -72,9 +78,10 @@ def report(label, pairs, w, h):
     where = [(i % w, i // w) for i in diff_hit.nonzero().flatten()[:4].tolist()]
     print(f"[order] {label}: Hit differs at {n_hit} of {w * h} pixels {where} (t {t.tolist()[:4]} vs in order {t_ref.tolist()[:4]}); "
           f"Linear at {n_lin}, Guide at {n_gui} (shaded from the same Hit)")
-    assert n_hit <= MAX_DIFFERING * w * h
+    max_hit, max_lin = MAX_DIFFERING[label]
+    assert n_hit <= max_hit
     assert bool((t <= t_ref).all()), "where the hits differ the batched pass must hold the nearer one"
-    assert n_lin <= MAX_DIFFERING * w * h and n_gui == 0
+    assert n_lin <= max_lin and n_gui == 0
 
 
 @pytest.mark.parametrize("frames", [1, 24])

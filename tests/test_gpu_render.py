@@ -8,7 +8,7 @@ Tolerances (stated by the comparison contract):
     the SDF march or the Newton solve settles on another point of the same
     primitive, and are reported with the ID mismatches;
   - radiance: |Linear_gpu - Linear_cpu| <= 2e-3 * max(1, |Linear_cpu|) on
-    >= 99.5% of pixels whose hit IDs agree; Pixels within 1 LSB there;
+    >= 99.9% of pixels whose hit IDs agree; Pixels within 1 LSB there;
   - filterLighting / resolvePixels on identical inputs: Filtered and History
     bit-exact, Pixels within 1 LSB (pow(x, 1/2.2) may round differently).
 Differences come only from CUDA's single-precision transcendentals in the
@@ -123,8 +123,15 @@ def test_fp64_rerun_on_mismatching_pixels(cuda, oracle, oracle64, scenes, gu, fo
     cpu_side = np.mean(r[:, 1] == f64[:, 1])
     gpu_err = np.max(np.abs(np.minimum(g[:, 0], 1e5) - np.minimum(f64[:, 0], 1e5)))
     cpu_err = np.max(np.abs(np.minimum(r[:, 0], 1e5) - np.minimum(f64[:, 0], 1e5)))
+    g_same = (g[:, 1] == f64[:, 1]) & (g[:, 2] == f64[:, 2])
+    lim = 2e-3 + 1e-4 * np.minimum(f64[:, 0], 1e5)
+    g_err_all = np.abs(np.minimum(g[:, 0], 1e5) - np.minimum(f64[:, 0], 1e5))
     print(f"[fp64 rerun] {len(bad)} mismatching px ({int(id_bad.sum())} id, {int(t_bad.sum())} t); FP64 id equals GPU on "
-          f"{gpu_side:.2f}, CPU on {cpu_side:.2f}; worst |t - t64| GPU {gpu_err:.4g} CPU {cpu_err:.4g}")
+          f"{gpu_side:.2f}, CPU on {cpu_side:.2f}; worst |t - t64| GPU {gpu_err:.4g} CPU {cpu_err:.4g}; "
+          f"GPU on the FP64 surface: worst {g_err_all[g_same].max() if g_same.any() else 0:.4g}")
+    # Where the GPU hits the primitive the FP64 rerun hits, its t is the FP64 t
+    # within the harness's BVH tolerance (2e-3 m, widened by 1e-4 t).
+    assert np.all(g_err_all[g_same] <= lim[g_same])
 
 
 @pytest.mark.parametrize("light", [0, 1])
@@ -143,10 +150,37 @@ def test_shade_forest_same_hits(cuda, oracle, scenes, gu, forest, view, light):
     errG = np.max(np.abs(G[:, :3] - Gr[:, :3]), 1)
     frac = np.mean(errL <= 2e-3)
     print(f"[shade view {view} light {light}] radiance within 2e-3 on {frac:.5f}; albedo max err {errG.max():.3g}")
-    assert frac >= 0.995
-    assert np.mean(errG <= 2e-3) >= 0.995
+    assert frac >= 0.999
+    assert np.mean(errG <= 2e-3) >= 0.999
     assert (L[:, 3] == 1).all() and (G[:, 3] == 1).all()
     assert np.isfinite(L).all() and (L >= 0).all()
+
+
+@pytest.mark.parametrize("view", [1, 2, 5])
+def test_gbuffer_normal_against_oracle(cuda, oracle, scenes, gu, forest, view):
+    """arbor_shadeGBuffer: Linear and Guide as arbor_shadePixels writes them,
+    and the Normal buffer equal to the normal shadePixels computes
+    (objectNormal in world space, facing the camera; the ground's noise
+    normal; zero for sky; Arbor.cu:231-234, 278-280) within 2e-3 per
+    component on >= 99.9 % of pixels (bark relief and leaf height use CUDA's
+    single-precision sinf/expf, glibc's on the CPU)."""
+    w, h = 160, 96
+    C = forest_camera(view, w, h, light=1)
+    s = scenes(1788)
+    hit = oracle.trace(s, C, w, h)
+    dC, dhit = gu.dev(C), gu.dev(hit)
+    lin, gui, nrm = gu.zeros_f(w * h * 4), gu.zeros_f(w * h * 4), gu.zeros_f(w * h * 4)
+    gu.ok(cuda.call("arbor_shadeGBuffer", forest.P, forest.Nodes, forest.Order, dC, dhit, lin, gui, nrm, w, h))
+    lin2, gui2 = gu.zeros_f(w * h * 4), gu.zeros_f(w * h * 4)
+    gu.ok(cuda.call("arbor_shadePixels", forest.P, forest.Nodes, forest.Order, dC, dhit, lin2, gui2, w, h))
+    assert np.array_equal(gu.host(lin), gu.host(lin2)) and np.array_equal(gu.host(gui), gu.host(gui2))
+    got = gu.host(nrm).reshape(-1, 4)
+    want = oracle.shade_normals(s, C, hit, w, h).reshape(-1, 4)
+    err = np.abs(got[:, :3] - want[:, :3]).max(1)
+    sky = hit.reshape(-1, 4)[:, 0] >= 1e5
+    print(f"[gbuffer normal view {view}] within 2e-3 on {np.mean(err <= 2e-3):.5f}; max err {err.max():.3g}")
+    assert np.mean(err <= 2e-3) >= 0.999
+    assert (got[sky, :3] == 0).all() and (got[:, 3] == 0).all()
 
 
 def test_shade_debug_modes(cuda, oracle, scenes, gu, forest):
@@ -159,7 +193,8 @@ def test_shade_debug_modes(cuda, oracle, scenes, gu, forest):
         lin, gui = gu.zeros_f(w * h * 4), gu.zeros_f(w * h * 4)
         gu.ok(cuda.call("arbor_shadePixels", forest.P, forest.Nodes, forest.Order, gu.dev(C), gu.dev(hit), lin, gui, w, h))
         err = np.abs(gu.host(lin) - lin_ref).reshape(-1, 4).max(1)
-        assert np.mean(err <= 2e-3) >= 0.995, f"mode {mode}"
+        print(f"[debug mode {mode}] within 2e-3 on {np.mean(err <= 2e-3):.5f}")
+        assert np.mean(err <= 2e-3) >= 0.999, f"mode {mode}"
 
 
 def test_shade_single_tree_shadows(cuda, oracle, scenes, gu, tree):
@@ -174,7 +209,8 @@ def test_shade_single_tree_shadows(cuda, oracle, scenes, gu, tree):
     lin, gui = gu.zeros_f(w * h * 4), gu.zeros_f(w * h * 4)
     gu.ok(cuda.call("arbor_shadeTreePixels", tree.P, tree.Nodes, tree.Order, gu.dev(C), gu.dev(hit), lin, gui, w, h))
     err = np.abs(gu.host(lin) - lin_ref).reshape(-1, 4).max(1)
-    assert np.mean(err <= 2e-3) >= 0.995
+    print(f"[single tree shadows] within 2e-3 on {np.mean(err <= 2e-3):.5f}")
+    assert np.mean(err <= 2e-3) >= 0.999
 
 
 @pytest.mark.parametrize("count", [0, 3])
@@ -226,7 +262,7 @@ def test_full_hd_frame_properties(cuda, oracle, scenes, gu, forest):
     idx = rng.choice(w * h, 2000, replace=False)
     xy = np.stack([idx % w, idx // w], 1).astype(np.int32)
     want = oracle.trace_pixel_list(scenes(1788), C, w, h, xy).reshape(-1, 4)[idx]
-    assert np.mean(hits[idx, 1] == want[:, 1]) >= 0.995
+    assert np.mean(hits[idx, 1] == want[:, 1]) >= ID_AGREEMENT
 
 
 def test_progressive_wind_shadows_4spp(cuda, oracle, scenes, gu):
