@@ -93,6 +93,8 @@ SIGNATURES = {
     "arbor_filterResolve": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_trace_work_slots": (ctypes.c_size_t, [_i, _i]),
     "arbor_forestInstances": (_i, [_i, _vp, _vp]),
+    "arbor_traceSpeciesPixels": (_i, [_vp, _vp, _vp, _i, ctypes.POINTER(_i), _vp, _vp, _i, _i, _vp]),
+    "arbor_shadeSpeciesPixels": (_i, [_vp, _vp, _vp, _i, ctypes.POINTER(_i), _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "arbor_tracePixelsInOrder": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
     "arbor_shadePixelsInOrder": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
     "arbor_traceWork": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp]),

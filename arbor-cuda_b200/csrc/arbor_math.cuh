@@ -184,7 +184,7 @@ struct Instance {
   float wc, wsn;   // cos/sin of +yaw (local normal -> world)
   float phase;     // wind phase
   int seed;        // forestSeed
-  int pad;
+  int species;     // scene of this instance in a forest of several species (0: the one resident scene)
 };
 __device__ __forceinline__ Instance make_instance(int tree, int ws) {
   Instance t;
@@ -202,7 +202,7 @@ __device__ __forceinline__ Instance make_instance(int tree, int ws) {
   t.wsn = xsin(yaw);
   t.seed = forest_seed(tree, ws);
   t.phase = (float)(t.seed & 8191) * 0.0017f;
-  t.pad = 0;
+  t.species = 0;
   return t;
 }
 // Arbor.cu:67-69

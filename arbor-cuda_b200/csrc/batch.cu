@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kBlock, 4) batch_compose_kernel(const BatchVie
   }
 }
 
-__global__ void __launch_bounds__(kFX * kFY) batch_filter_kernel(const BatchView* __restrict__ views, const float4* __restrict__ scal,
+__global__ void __launch_bounds__(kFX * kFT) batch_filter_kernel(const BatchView* __restrict__ views, const float4* __restrict__ scal,
                                                                  const int4* __restrict__ tiles, int n_tiles, int* __restrict__ counter) {
   __shared__ FilterTile s;
   __shared__ int s_tile;
@@ -307,7 +307,7 @@ int configure(arbor_batch* b, const arbor_batch_config& cfg) {
   int st = launch_setup(b, b->own);
   if (!st) st = launch_trace_shade(b, cfg, b->tiles, b->n_ts, b->n_views, b->own);
   if (!st) {
-    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFY), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter,
+    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFT), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter,
                                                                    b->counters + kQueueFilter);
     st = check_launch("batch_filter_kernel");
   }
@@ -568,7 +568,7 @@ extern "C" int arbor_batch_profile(arbor_batch* b, float* ms4) {
     cudaEventRecord(ev[3], b->own);
   }
   if (status == ARBOR_OK) {
-    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFY), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter,
+    batch_filter_kernel<<<b->sms * 8, dim3(kFX, kFT), 0, b->own>>>(b->views, b->scal, b->tiles + b->n_ts, b->n_filter,
                                                                    b->counters + kQueueFilter);
     status = check_launch("batch_filter_kernel");
     cudaEventRecord(ev[4], b->own);

@@ -373,7 +373,7 @@ struct ShadowPolicy {
     int id = (int)r.found;
     if (id < 0) {
       write(trans);
-    } else if (ldg4(ctx->P, id * 6).w != 1.0f) {
+    } else if (ldg4(scene_P(*ctx, ctx->species && r.foundTree >= 0 ? ctx->inst[r.foundTree].species : 0), id * 6).w != 1.0f) {
       write(mk(0.0f, 0.0f, 0.0f));
     } else {
       trans = trans * mk(0.18f, 0.29f, 0.065f);
@@ -427,7 +427,7 @@ struct StagedShadowPolicy {
     int id = (int)r.found;
     if (id < 0) {
       write(trans);
-    } else if (ldg4(ctx->P, id * 6).w != 1.0f) {
+    } else if (ldg4(scene_P(*ctx, ctx->species && r.foundTree >= 0 ? ctx->inst[r.foundTree].species : 0), id * 6).w != 1.0f) {
       write(mk(0.0f, 0.0f, 0.0f));
     } else {
       trans = trans * mk(0.18f, 0.29f, 0.065f);
@@ -466,13 +466,19 @@ __device__ __forceinline__ void staged_shadow_pool(const TraceCtx& c, WB& b, con
 }
 
 // shadePixels' colour of pixel (x, y) (Arbor.cu:277-289), its visibility
-// read from Linear where the shadow pass traced one.
-template <bool kForestScene>
+// read from Linear where the shadow pass traced one.  kSpecies: a forest of
+// several species, P holding one scene per species back to back; the hit
+// instance's scene is shaded.
+template <bool kForestScene, bool kSpecies = false>
 __device__ __forceinline__ void shade_compose_px(const float* __restrict__ P, const Camera& cam, const Instance* inst, const float* __restrict__ Hit,
                                                  float* __restrict__ Linear, float* __restrict__ Guide, float* __restrict__ Normal, int x, int y,
                                                  int width, int height) {
   const int pixel = y * width + x;
   const float4 hit = __ldg(reinterpret_cast<const float4*>(Hit) + pixel);
+  if (kSpecies) {
+    const int tree = (int)hit.z;
+    if (tree >= 0 && tree < kForest) P += (size_t)inst[tree].species * (kCapacity * kPS);
+  }
   Shading sh;
   shade_pre<kForestScene>(P, cam, inst, hit, x, y, width, height, sh);
   f3 vis = mk(1.0f, 1.0f, 1.0f);
@@ -484,26 +490,35 @@ __device__ __forceinline__ void shade_compose_px(const float* __restrict__ P, co
 }
 
 // ------------------------------------------------------ filter / resolve --
-constexpr int kFX = 32, kFY = 8, kHalo = 2;
+// A filter tile is kFX x kFY output pixels, computed by kFX x kFT threads
+// (threadIdx.x, threadIdx.y), each thread a vertical pair of pixels.
+constexpr int kFX = 32, kFY = 16, kFT = kFY / 2, kHalo = 2;
 constexpr int kSX = kFX + 2 * kHalo, kSY = kFY + 2 * kHalo;
 
 // Arbor.cu:303
 __device__ __forceinline__ float aces(float x) { return sat((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f)); }
 
 // One channel of resolvePixels' output byte (Arbor.cu:304, packRGB :49):
-// (uint)(sat(pow(c, 1/2.2) * vig) * 255 + 0.5).  The power is the float of
-// the double-precision pow (xpow); CUDA's single-precision powf is within a
-// few ulp of it, which moves the byte only when the scaled value lies within
-// about 1e-4 of a rounding boundary, so powf's byte is used unless the value
-// is within 1e-3 of one, where xpow decides.  Same bytes, cheaper on average.
+// byte = (uint)(t), t = sat(pow(aces(c), 1/2.2) * vig) * 255 + 0.5, with the
+// power taken as the float of the double-precision pow (xpow) and aces with
+// IEEE division.  The byte changes only where t crosses an integer.  The fast
+// path evaluates t with an approximate division in aces (within 2 ulp) and
+// the hardware exp2/log2 power (__powf: relative error below 1e-6 wherever
+// the power is above 1e-3, and an absolute error below 1e-9 under it), so its
+// t is within 3e-4 of the exact t; where it lies within 1e-3 of an integer
+// the exact t decides.  Same bytes as the exact evaluation, far fewer
+// instructions.
 __device__ __forceinline__ uint32_t gamma_byte(float c, float vig) {
-  float t = sat(powf(c, 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
+  const float a = sat(__fdividef(c * (2.51f * c + 0.03f), c * (2.43f * c + 0.59f) + 0.14f));
+  float t = sat(__powf(a, 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
   const float fr = t - floorf(t);
-  if (fr < 1e-3f || fr > 1.0f - 1e-3f) t = sat(xpow(c, 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
+  // (|c| >= 1e18 also takes the exact path: there the approximate division's
+  // denominator can pass 2^126, where __fdividef returns 0.)
+  if (fr < 1e-3f || fr > 1.0f - 1e-3f || !(fabsf(c) < 1e18f)) t = sat(xpow(aces(c), 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
   return (uint32_t)t;
 }
 
-// Arbor.cu:304, one pixel.
+// Arbor.cu:304, one pixel: `current` is the filtered colour.
 __device__ __forceinline__ void resolve_px(f3 current, float* __restrict__ History, uint32_t* __restrict__ Pixels, float c9, float c10,
                                            float exposure, int x, int y, int width, int height) {
   int i = y * width + x;
@@ -511,49 +526,117 @@ __device__ __forceinline__ void resolve_px(f3 current, float* __restrict__ Histo
   f3 mean = current;
   if (!(count < 0.5f)) mean = mix3(xyz(reinterpret_cast<const float4*>(History)[i]), current, 1.0f / (count + 1.0f));
   reinterpret_cast<float4*>(History)[i] = make_float4(mean.x, mean.y, mean.z, count + 1.0f);
-  f3 col = mean * exposure;
-  col = mk(aces(col.x), aces(col.y), aces(col.z));
+  const f3 col = mean * exposure;
   float u = ((float)x / (float)width - 0.5f) * 2.0f;
   float v = ((float)y / (float)height - 0.5f) * 2.0f;
   const float vig = 1.0f - 0.09f * (u * u + v * v);
   Pixels[i] = gamma_byte(col.x, vig) | (gamma_byte(col.y, vig) << 8) | (gamma_byte(col.z, vig) << 16) | 4278190080u;
 }
 
-// Same-surface 5x5 demodulated filter (Arbor.cu:292-302) of one 32x8 tile,
-// staged with a 2-pixel halo in shared memory so each input pixel is read
-// from HBM once per tile.  Each halo pixel is staged once as its same-surface
-// key (depth, (int) primitive id, (int) tree id) and its demodulated colour
-// Linear / (Guide + 0.02): the same conversions and IEEE quotients the
-// reference evaluates per neighbour, evaluated once per pixel.  The 5x5 loop
-// is unrolled in the reference's order (rows, then columns) with its weights
-// as constants; tiles whose halo lies inside the image skip the bounds test.
-// kResolve fuses resolvePixels on the filtered value.  Threads are laid out
-// 32 x 8 (threadIdx.x, threadIdx.y).
+// Same-surface 5x5 demodulated filter (Arbor.cu:292-302) of one kFX x kFY
+// tile, staged with a 2-pixel halo in shared memory so each input pixel is
+// read from HBM once per tile.  Each halo pixel is staged once as its depth,
+// its surface key and its demodulated colour Linear / (Guide + 0.02): the
+// same conversions and IEEE quotients the reference evaluates per neighbour,
+// evaluated once per pixel.  The surface key packs (int) primitive id + 1 and
+// (int) tree id + 1 into 16 bits each, so one integer compare decides "same
+// primitive and same tree"; a tile holding an id or tree id outside
+// -1..65534 (never written by tracePixels) is filtered by the reference's
+// per-neighbour loop instead (filter_px_direct).  Each thread filters a
+// vertical pair of pixels: their 5x5 windows share 20 taps, loaded once.
+// Each pixel's taps are accumulated in the reference's order (rows, then
+// columns) with its weights as constants; tiles whose halo lies inside the
+// image skip the bounds test.  kResolve fuses resolvePixels on the filtered
+// value.
 struct FilterTile {
-  int4 key[kSY][kSX];      // depth bits, primitive id, tree id
+  int2 key[kSY][kSX];      // depth bits, packed surface key
   float4 demod[kSY][kSX];  // Linear / (Guide + 0.02)
   float w[6];              // weights of r^2 = 0, 1, 2, 4, 5, 8
 };
 
+// Weight of tap (j, k), from the staged exp(-0.3 r^2) values (compile-time index).
+__device__ __forceinline__ float tap_weight(const float (&w)[6], int j, int k) {
+  const int r2 = j * j + k * k;
+  return w[r2 == 0 ? 0 : r2 == 1 ? 1 : r2 == 2 ? 2 : r2 == 4 ? 3 : r2 == 5 ? 4 : 5];
+}
+
+// The centre pixel of a filter pass and its running sums.
+struct FilterCentre {
+  int key;
+  float depth, tol;
+  f3 sum;
+  float weight;
+};
+
+// One tap of one centre: accept a neighbour with the same surface key and
+// |depth difference| not above the tolerance (Arbor.cu:297-299).
+__device__ __forceinline__ void filter_tap(FilterCentre& c, int2 q, const float4* demod, float wt) {
+  if (q.y != c.key || fabsf(__int_as_float(q.x) - c.depth) > c.tol) return;
+  const float4 d = *demod;
+  c.sum = c.sum + mk(d.x, d.y, d.z) * wt;
+  c.weight += wt;
+}
+
+// The taps of a vertical pixel pair centred at shared-memory (cx, cy) and
+// (cx, cy + 1), image (x, y) and (x, y + 1): rows cy - 2 .. cy + 3 are read
+// once; row r feeds pixel 0 as tap row r - cy and pixel 1 as tap row
+// r - cy - 1.
 template <bool kEdge>
-__device__ __forceinline__ void filter_gather(const FilterTile& s, int cx, int cy, int x, int y, int width, int height, int id, int tree,
-                                              float depth, float tol, const float (&w)[6], f3& sum, float& weight) {
+__device__ __forceinline__ void filter_pair(const FilterTile& s, int cx, int cy, int x, int y, int width, int height, const float (&w)[6],
+                                            FilterCentre& p0, FilterCentre& p1, bool live0, bool live1) {
 #pragma unroll
-  for (int j = -2; j <= 2; j++)
+  for (int r = -2; r <= 3; r++)
 #pragma unroll
     for (int k = -2; k <= 2; k++) {
+      const int2 q = s.key[cy + r][cx + k];
+      const float4* d = &s.demod[cy + r][cx + k];
       if (kEdge) {
-        int xx = x + k, yy = y + j;
-        if (xx < 0 || yy < 0 || xx >= width || yy >= height) continue;
+        const int xx = x + k, yy = y + r;
+        if (xx < 0 || xx >= width || yy < 0 || yy >= height) continue;
       }
-      const int4 q = s.key[cy + j][cx + k];
-      if (q.y != id || q.z != tree || fabsf(__int_as_float(q.x) - depth) > tol) continue;
-      const int r2 = j * j + k * k;
-      const float wt = w[r2 == 0 ? 0 : r2 == 1 ? 1 : r2 == 2 ? 2 : r2 == 4 ? 3 : r2 == 5 ? 4 : 5];
-      const float4 d = s.demod[cy + j][cx + k];
-      sum = sum + mk(d.x, d.y, d.z) * wt;
+      if (r <= 2 && live0) filter_tap(p0, q, d, tap_weight(w, r, k));
+      if (r >= -1 && live1) filter_tap(p1, q, d, tap_weight(w, r - 1, k));
+    }
+}
+
+// filterLighting of pixel (x, y) straight from global memory, in the
+// reference's per-neighbour form (Arbor.cu:292-302): the path for tiles whose
+// ids do not fit the packed key.
+__device__ __noinline__ f3 filter_px_direct(const float* __restrict__ Linear, const float* __restrict__ Guide, const float* __restrict__ Hit,
+                                            int x, int y, int width, int height) {
+  const int i = y * width + x;
+  const float4 lc = __ldg(reinterpret_cast<const float4*>(Linear) + i);
+  const float4 gc = __ldg(reinterpret_cast<const float4*>(Guide) + i);
+  const float4 hc = __ldg(reinterpret_cast<const float4*>(Hit) + i);
+  f3 col = mk(lc.x, lc.y, lc.z);
+  const f3 base = mk(gc.x, gc.y, gc.z) + mk(0.02f, 0.02f, 0.02f);
+  f3 sum = mk(0.0f, 0.0f, 0.0f);
+  float weight = 0.0f;
+  const int id = (int)hc.y, tree = (int)hc.z;
+  const float tol = fmaxf(0.005f, hc.w * 6.0f);
+  for (int j = -2; j <= 2; j++)
+    for (int k = -2; k <= 2; k++) {
+      const int xx = x + k, yy = y + j;
+      if (xx < 0 || yy < 0 || xx >= width || yy >= height) continue;
+      const int q = yy * width + xx;
+      const float4 h = __ldg(reinterpret_cast<const float4*>(Hit) + q);
+      if ((int)h.y != id || (int)h.z != tree || fabsf(h.x - hc.x) > tol) continue;
+      const float wt = xexp(-(float)(j * j + k * k) * 0.30f);  // the staged weights' values
+      const float4 l = __ldg(reinterpret_cast<const float4*>(Linear) + q);
+      const float4 g = __ldg(reinterpret_cast<const float4*>(Guide) + q);
+      sum = sum + mk(l.x / (g.x + 0.02f), l.y / (g.y + 0.02f), l.z / (g.z + 0.02f)) * wt;
       weight += wt;
     }
+  if (weight > 0.0f) col = mix3(col, (sum / weight) * base, 0.86f);
+  return col;
+}
+
+// Packed surface key of a Hit record, or -1 (never a packed key) when its
+// ids lie outside -1..65534.
+__device__ __forceinline__ int surface_key(float id_f, float tree_f) {
+  const int id = (int)id_f, tree = (int)tree_f;
+  if (id < -1 || id > 65534 || tree < -1 || tree > 65534) return -1;
+  return (id + 1) | ((tree + 1) << 16);
 }
 
 template <bool kResolve>
@@ -568,43 +651,80 @@ __device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restri
     s.w[tid] = xexp(-(float)r2[tid] * 0.30f);
   }
   const int hx0 = x0 - kHalo, hy0 = y0 - kHalo;
-  for (int k = tid; k < kSX * kSY; k += kFX * kFY) {
-    int sy = k / kSX, sx = k - sy * kSX;
-    int gx = hx0 + sx, gy = hy0 + sy;
+  bool unpacked = false;
+  for (int k = tid; k < kSX * kSY; k += kFX * kFT) {
+    const int sy = k / kSX, sx = k - sy * kSX;
+    const int gx = hx0 + sx, gy = hy0 + sy;
     if (gx >= 0 && gy >= 0 && gx < width && gy < height) {
-      int q = gy * width + gx;
-      float4 h = __ldg(reinterpret_cast<const float4*>(Hit) + q);
-      float4 l = __ldg(reinterpret_cast<const float4*>(Linear) + q);
-      float4 g = __ldg(reinterpret_cast<const float4*>(Guide) + q);
-      s.key[sy][sx] = make_int4(__float_as_int(h.x), (int)h.y, (int)h.z, 0);
+      const int q = gy * width + gx;
+      const float4 h = __ldg(reinterpret_cast<const float4*>(Hit) + q);
+      const float4 l = __ldg(reinterpret_cast<const float4*>(Linear) + q);
+      const float4 g = __ldg(reinterpret_cast<const float4*>(Guide) + q);
+      const int key = surface_key(h.y, h.z);
+      unpacked |= key < 0;
+      s.key[sy][sx] = make_int2(__float_as_int(h.x), key);
       s.demod[sy][sx] = make_float4(l.x / (g.x + 0.02f), l.y / (g.y + 0.02f), l.z / (g.z + 0.02f), 0.0f);
     }
   }
-  __syncthreads();
-  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-  if (x < width && y < height) {
-    const int cx = threadIdx.x + kHalo, cy = threadIdx.y + kHalo;
-    const int i = y * width + x;
-    const int4 kc = s.key[cy][cx];
-    const float depth = __int_as_float(kc.x);
-    float4 lc = __ldg(reinterpret_cast<const float4*>(Linear) + i);
-    f3 col = mk(lc.x, lc.y, lc.z);
-    if (depth < kFar && c15 < 0.5f) {
-      float4 gc = __ldg(reinterpret_cast<const float4*>(Guide) + i);
-      f3 base = mk(gc.x, gc.y, gc.z) + mk(0.02f, 0.02f, 0.02f);
-      f3 sum = mk(0.0f, 0.0f, 0.0f);
-      float weight = 0.0f;
-      const float tol = fmaxf(0.005f, __ldg(Hit + 4 * i + 3) * 6.0f);
-      const float w[6] = {s.w[0], s.w[1], s.w[2], s.w[3], s.w[4], s.w[5]};
-      const bool interior = x0 >= kHalo && y0 >= kHalo && x0 + kFX + kHalo <= width && y0 + kFY + kHalo <= height;
+  unpacked = __syncthreads_or(unpacked);
+  const float w[6] = {s.w[0], s.w[1], s.w[2], s.w[3], s.w[4], s.w[5]};
+  const int x = x0 + threadIdx.x, y = y0 + 2 * threadIdx.y;
+  if (x >= width || y >= height) return;
+  const int cx = threadIdx.x + kHalo, cy = 2 * threadIdx.y + kHalo;
+  const bool has1 = y + 1 < height;
+  const int i0 = y * width + x, i1 = i0 + width;
+  const bool filter = c15 < 0.5f;
+  FilterCentre p[2];
+  bool live[2];
+#pragma unroll
+  for (int e = 0; e < 2; e++) {
+    const int2 kc = s.key[cy + e][cx];
+    p[e].key = kc.y;
+    p[e].depth = __int_as_float(kc.x);
+    p[e].sum = mk(0.0f, 0.0f, 0.0f);
+    p[e].weight = 0.0f;
+    live[e] = filter && (e == 0 || has1) && p[e].depth < kFar;
+    p[e].tol = live[e] ? fmaxf(0.005f, __ldg(Hit + 4 * (e ? i1 : i0) + 3) * 6.0f) : 0.0f;
+  }
+  f3 col[2];
+  if (!unpacked) {
+    const bool interior = x0 >= kHalo && y0 >= kHalo && x0 + kFX + kHalo <= width && y0 + kFY + kHalo <= height;
+    if (live[0] || live[1]) {
       if (interior)
-        filter_gather<false>(s, cx, cy, x, y, width, height, kc.y, kc.z, depth, tol, w, sum, weight);
+        filter_pair<false>(s, cx, cy, x, y, width, height, w, p[0], p[1], live[0], live[1]);
       else
-        filter_gather<true>(s, cx, cy, x, y, width, height, kc.y, kc.z, depth, tol, w, sum, weight);
-      if (weight > 0.0f) col = mix3(col, (sum / weight) * base, 0.86f);
+        filter_pair<true>(s, cx, cy, x, y, width, height, w, p[0], p[1], live[0], live[1]);
     }
-    reinterpret_cast<float4*>(Filtered)[i] = make_float4(col.x, col.y, col.z, 1.0f);
-    if (kResolve) resolve_px(col, History, Pixels, c9, c10, c20, x, y, width, height);
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      if (e == 1 && !has1) break;
+      const int i = e ? i1 : i0;
+      const float4 lc = __ldg(reinterpret_cast<const float4*>(Linear) + i);
+      col[e] = mk(lc.x, lc.y, lc.z);
+      if (live[e] && p[e].weight > 0.0f) {
+        const float4 gc = __ldg(reinterpret_cast<const float4*>(Guide) + i);
+        const f3 base = mk(gc.x, gc.y, gc.z) + mk(0.02f, 0.02f, 0.02f);
+        col[e] = mix3(col[e], (p[e].sum / p[e].weight) * base, 0.86f);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      if (e == 1 && !has1) break;
+      const int i = e ? i1 : i0;
+      if (live[e]) {
+        col[e] = filter_px_direct(Linear, Guide, Hit, x, y + e, width, height);
+      } else {
+        const float4 lc = __ldg(reinterpret_cast<const float4*>(Linear) + i);
+        col[e] = mk(lc.x, lc.y, lc.z);
+      }
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 2; e++) {
+    if (e == 1 && !has1) break;
+    reinterpret_cast<float4*>(Filtered)[e ? i1 : i0] = make_float4(col[e].x, col[e].y, col[e].z, 1.0f);
+    if (kResolve) resolve_px(col[e], History, Pixels, c9, c10, c20, x, y + e, width, height);
   }
 }
 

@@ -86,6 +86,71 @@ __global__ void __launch_bounds__(kBlock, 4) shade_compose_kernel(const float* _
   if (x < width && y < height) shade_compose_px<kForestScene>(P, cam, inst, Hit, Linear, Guide, Normal, x, y, width, height);
 }
 
+// ------------------------------------------------ forest of several species --
+// The reference's 324 instances all share one resident tree (README.md:8,
+// docs/ARCHITECTURE.md:5).  These kernels trace and shade a forest whose
+// instance t keeps the reference's transform, wind phase and tint but takes
+// its geometry (its own records and BVH) from scene of[t]; P, Nodes and Order
+// hold the scenes back to back.  The 2D DDA, bounding spheres and every
+// per-instance step are the reference's; only the scene a tree's traversal
+// and tests read changes.  With every of[t] = 0 the results equal
+// arbor_tracePixels / arbor_shadePixels on scene 0.
+struct SpeciesMap {
+  uint8_t of[kForest];
+};
+__device__ __forceinline__ void species_setup(Instance* inst, const SpeciesMap& m) {
+  for (int t = threadIdx.x; t < kForest; t += blockDim.x) inst[t].species = m.of[t];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBlock, 2) trace_species_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                                  const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                                  float* __restrict__ Hit, int width, int height, const SpeciesMap map) {
+  extern __shared__ float4 batch_smem[];
+  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForest];
+  __shared__ int next;
+  if (threadIdx.x == 0) next = 0;
+  block_setup(C, cam, inst, true);
+  species_setup(inst, map);
+  const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, true, true};
+  const int bx = (width + 7) / 8;
+  const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
+  trace_pool(c, cam, b, Hit, pool);
+}
+
+__global__ void __launch_bounds__(kBlock, 2) shadow_species_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
+                                                                   const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                                   const float* __restrict__ Guide, float* __restrict__ Linear, int width, int height,
+                                                                   const SpeciesMap map) {
+  extern __shared__ float4 batch_smem[];
+  WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForest];
+  __shared__ int next;
+  if (threadIdx.x == 0) next = 0;
+  block_setup(C, cam, inst, true);
+  if (!(cam.shadows > 0.5f)) return;
+  species_setup(inst, map);
+  const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, true, true};
+  const int bx = (width + 7) / 8;
+  const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
+  staged_shadow_pool(c, b, Guide, Linear, pool);
+}
+
+__global__ void __launch_bounds__(kBlock, 4) shade_compose_species_kernel(const float* __restrict__ P, const float* __restrict__ C,
+                                                                          const float* __restrict__ Hit, float* __restrict__ Linear,
+                                                                          float* __restrict__ Guide, int width, int height, const SpeciesMap map) {
+  __shared__ Camera cam;
+  __shared__ Instance inst[kForest];
+  block_setup(C, cam, inst, true);
+  species_setup(inst, map);
+  int x, y;
+  tile_pixel_at(threadIdx.x, blockIdx.x * kTile, blockIdx.y * kTile, kTile, x, y);
+  if (x < width && y < height) shade_compose_px<true, true>(P, cam, inst, Hit, Linear, Guide, nullptr, x, y, width, height);
+}
+
 // tracePixels and shadePixels with the reference's traversal as written
 // (Arbor.cu:220-289): one ray per thread over 16x16-pixel CTAs, candidates
 // tested in visiting order, children nearest entry first, no warp batching.
@@ -155,7 +220,7 @@ __global__ void __launch_bounds__(kBlock) shade_inorder_kernel(const float* __re
 }
 
 template <bool kResolve>
-__global__ void __launch_bounds__(kFX * kFY) filter_kernel(const float* __restrict__ Linear, const float* __restrict__ Guide,
+__global__ void __launch_bounds__(kFX * kFT, 3) filter_kernel(const float* __restrict__ Linear, const float* __restrict__ Guide,
                                                            const float* __restrict__ Hit, float* __restrict__ Filtered,
                                                            float* __restrict__ History, uint32_t* __restrict__ Pixels,
                                                            const float* __restrict__ C, int width, int height) {
@@ -164,11 +229,12 @@ __global__ void __launch_bounds__(kFX * kFY) filter_kernel(const float* __restri
                         kResolve ? C[20] : 0.0f, width, height, blockIdx.x * kFX, blockIdx.y * kFY);
 }
 
-// resolvePixels alone (Arbor.cu:304).
-__global__ void __launch_bounds__(kFX * kFY) resolve_kernel(const float* __restrict__ Filtered, float* __restrict__ History,
+// resolvePixels alone (Arbor.cu:304): 32x8-pixel CTAs, one pixel per thread.
+constexpr int kRX = 32, kRY = 8;
+__global__ void __launch_bounds__(kRX * kRY) resolve_kernel(const float* __restrict__ Filtered, float* __restrict__ History,
                                                             uint32_t* __restrict__ Pixels, const float* __restrict__ C, int width,
                                                             int height) {
-  const int x = blockIdx.x * kFX + threadIdx.x, y = blockIdx.y * kFY + threadIdx.y;
+  const int x = blockIdx.x * kRX + threadIdx.x, y = blockIdx.y * kRY + threadIdx.y;
   if (x >= width || y >= height) return;
   float4 f = __ldg(reinterpret_cast<const float4*>(Filtered) + y * width + x);
   resolve_px(mk(f.x, f.y, f.z), History, Pixels, C[9], C[10], C[20], x, y, width, height);
@@ -206,6 +272,7 @@ dim3 pool_grid(int w, int h) {
   return dim3((unsigned)std::min<long>(blocks, 2L * sms[dev]));
 }
 dim3 filter_grid(int w, int h) { return dim3((w + kFX - 1) / kFX, (h + kFY - 1) / kFY); }
+dim3 resolve_grid(int w, int h) { return dim3((w + kRX - 1) / kRX, (h + kRY - 1) / kRY); }
 
 int trace_entry(const char* name, bool forest, const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width,
                 int height, cudaStream_t stream) {
@@ -263,10 +330,79 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
   return check_launch(name);
 }
 
+// Checks of a forest-of-species call: 1..256 scenes, every instance on one
+// of them.  Fills `map`.
+int species_args(const char* name, int n_species, const int* species_of, SpeciesMap& map) {
+  if (n_species < 1 || n_species > ARBOR_MAX_SPECIES) {
+    set_error("%s: n_species %d outside 1..%d", name, n_species, ARBOR_MAX_SPECIES);
+    return ARBOR_ERR_VALUE;
+  }
+  if (species_of == nullptr) {
+    set_error("%s: species_of is NULL", name);
+    return ARBOR_ERR_NULL;
+  }
+  for (int t = 0; t < kForest; t++) {
+    if (species_of[t] < 0 || species_of[t] >= n_species) {
+      set_error("%s: species_of[%d] = %d outside 0..%d", name, t, species_of[t], n_species - 1);
+      return ARBOR_ERR_VALUE;
+    }
+    map.of[t] = (uint8_t)species_of[t];
+  }
+  return ARBOR_OK;
+}
+
 }  // namespace
 }  // namespace arbor
 
 using namespace arbor;
+
+extern "C" int arbor_traceSpeciesPixels(const float* P, const float* Nodes, const uint32_t* Order, int n_species, const int* species_of,
+                                        const float* C, float* Hit, int width, int height, arbor_stream stream) {
+  const char* name = "arbor_traceSpeciesPixels";
+  SpeciesMap map;
+  if (int s = species_args(name, n_species, species_of, map)) return s;
+  bool empty;
+  if (int s = check_image(name, width, height, &empty)) return s;
+  const size_t n = (size_t)n_species;
+  const Binding b[] = {{P, n * kP, false, 16, "P"},
+                       {Nodes, n * kNodes, false, 16, "Nodes"},
+                       {Order, n * kKeys, false, 4, "Order"},
+                       {C, kC, false, 4, "C"},
+                       {Hit, empty ? 0 : image_bytes(width, height), true, 16, "Hit"}};
+  if (int s = check_bindings(name, b)) return s;
+  if (empty) return ARBOR_OK;
+  if (!batch_smem_ready((const void*)trace_species_kernel)) {
+    set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
+    return ARBOR_ERR_CUDA;
+  }
+  trace_species_kernel<<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height, map);
+  count_launch();
+  return check_launch(name);
+}
+extern "C" int arbor_shadeSpeciesPixels(const float* P, const float* Nodes, const uint32_t* Order, int n_species, const int* species_of,
+                                        const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, arbor_stream stream) {
+  const char* name = "arbor_shadeSpeciesPixels";
+  SpeciesMap map;
+  if (int s = species_args(name, n_species, species_of, map)) return s;
+  bool empty;
+  if (int s = check_image(name, width, height, &empty)) return s;
+  const size_t n = (size_t)n_species;
+  const size_t img = empty ? 0 : image_bytes(width, height);
+  const Binding b[] = {{P, n * kP, false, 16, "P"},  {Nodes, n * kNodes, false, 16, "Nodes"}, {Order, n * kKeys, false, 4, "Order"},
+                       {C, kC, false, 4, "C"},      {Hit, img, false, 16, "Hit"},             {Linear, img, true, 16, "Linear"},
+                       {Guide, img, true, 16, "Guide"}};
+  if (int s = check_bindings(name, b)) return s;
+  if (empty) return ARBOR_OK;
+  if (!batch_smem_ready((const void*)shadow_species_kernel)) {
+    set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
+    return ARBOR_ERR_CUDA;
+  }
+  shadow_setup_kernel<<<pixel_grid(width, height), kBlock, 0, stream>>>(C, Hit, Linear, Guide, width, height);
+  shadow_species_kernel<<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Guide, Linear, width, height, map);
+  shade_compose_species_kernel<<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, width, height, map);
+  count_launch(3);
+  return check_launch(name);
+}
 
 extern "C" int arbor_tracePixels(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height,
                                  arbor_stream stream) {
@@ -342,7 +478,7 @@ extern "C" int arbor_filterLighting(const float* Linear, const float* Guide, con
                        {C, kC, false, 4, "C"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
-  filter_kernel<false><<<filter_grid(width, height), dim3(kFX, kFY), 0, stream>>>(Linear, Guide, Hit, Filtered, nullptr, nullptr, C, width,
+  filter_kernel<false><<<filter_grid(width, height), dim3(kFX, kFT), 0, stream>>>(Linear, Guide, Hit, Filtered, nullptr, nullptr, C, width,
                                                                                   height);
   count_launch();
   return check_launch(name);
@@ -359,7 +495,7 @@ extern "C" int arbor_resolvePixels(const float* Filtered, float* History, uint32
                        {C, kC, false, 4, "C"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
-  resolve_kernel<<<filter_grid(width, height), dim3(kFX, kFY), 0, stream>>>(Filtered, History, Pixels, C, width, height);
+  resolve_kernel<<<resolve_grid(width, height), dim3(kRX, kRY), 0, stream>>>(Filtered, History, Pixels, C, width, height);
   count_launch();
   return check_launch(name);
 }
@@ -375,7 +511,7 @@ extern "C" int arbor_filterResolve(const float* Linear, const float* Guide, cons
                        {C, kC, false, 4, "C"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
-  filter_kernel<true><<<filter_grid(width, height), dim3(kFX, kFY), 0, stream>>>(Linear, Guide, Hit, Filtered, History, Pixels, C, width,
+  filter_kernel<true><<<filter_grid(width, height), dim3(kFX, kFT), 0, stream>>>(Linear, Guide, Hit, Filtered, History, Pixels, C, width,
                                                                                  height);
   count_launch();
   return check_launch(name);

@@ -46,6 +46,7 @@ struct Ray {
   uint32_t pending;
   float spanx;
   int phase;
+  int species;      // scene of the tree being traversed (forest of several species; 0 otherwise)
 };
 
 struct TraceCtx {
@@ -57,11 +58,21 @@ struct TraceCtx {
   bool refine;            // primary rays: wood refined by the SDF march, their own visiting order,
                           // ties settled by ref_before; false for shadow segments
   bool forest;            // false: the single-tree scene (identity instance)
+  bool species = false;   // true: a forest of several species, P / Nodes / Order holding one scene
+                          // per species back to back, instance t on scene inst[t].species
 };
 
-__device__ __forceinline__ void load_node(const TraceCtx& c, int n, float4& lo, float4& hi) {
-  lo = ldg4(c.Nodes, 2 * n);
-  hi = ldg4(c.Nodes, 2 * n + 1);
+// The records of scene `s` (s = 0 unless the forest has several species).
+__device__ __forceinline__ const float* scene_P(const TraceCtx& c, int s) { return c.species ? c.P + (size_t)s * (kCapacity * kPS) : c.P; }
+__device__ __forceinline__ const float* scene_nodes(const TraceCtx& c, int s) {
+  return c.species ? c.Nodes + (size_t)s * (kNodeCount * 8) : c.Nodes;
+}
+__device__ __forceinline__ const uint32_t* scene_order(const TraceCtx& c, int s) { return c.species ? c.Order + (size_t)s * kCapacity : c.Order; }
+
+__device__ __forceinline__ void load_node(const TraceCtx& c, const Ray& r, int n, float4& lo, float4& hi) {
+  const float* nodes = scene_nodes(c, r.species);
+  lo = ldg4(nodes, 2 * n);
+  hi = ldg4(nodes, 2 * n + 1);
 }
 
 // Tree entry with the root test (Arbor.cu:221-223).  Returns true when the
@@ -72,7 +83,7 @@ __device__ __forceinline__ bool enter_tree(const TraceCtx& c, Ray& r) {
   r.depth = 0;
   r.pending = 0u;
   float4 lo, hi;
-  load_node(c, 1, lo, hi);
+  load_node(c, r, 1, lo, hi);
   return node_accept(lo, hi, r.lro, r.linv, r.lbest, r.spanx);
 }
 
@@ -99,13 +110,13 @@ __device__ __forceinline__ void dda_advance(Ray& r) {
 __device__ __forceinline__ void finish_tree(const TraceCtx& c, Ray& r) {
   if (!c.forest) {
     r.best = r.lbest;
-    r.found = r.lfound >= 0 && c.refine ? (float)__ldg(c.Order + r.lfound) : (float)r.lfound;
+    r.found = r.lfound >= 0 && c.refine ? (float)__ldg(scene_order(c, r.species) + r.lfound) : (float)r.lfound;
     r.phase = kPhDone;
     return;
   }
   if (r.lfound >= 0 && r.lbest * r.lsc < r.best) {
     r.best = r.lbest * r.lsc;
-    r.found = c.refine ? (float)__ldg(c.Order + r.lfound) : (float)r.lfound;
+    r.found = c.refine ? (float)__ldg(scene_order(c, r.species) + r.lfound) : (float)r.lfound;
     r.foundTree = r.tree;
   }
   dda_advance(r);
@@ -119,6 +130,7 @@ __device__ __forceinline__ void ray_begin(const TraceCtx& c, Ray& r, f3 ro, f3 r
   r.found = -1.0f;
   r.foundTree = -1;
   r.tree = -1;
+  r.species = 0;
   if (!c.forest) {
     r.lro = ro;
     r.lrd = rd;
@@ -176,6 +188,7 @@ __device__ __forceinline__ void dda_step(const TraceCtx& c, Ray& r) {
     r.lbest = r.best / it.sc;
     r.ltime = c.time + it.phase;
     r.lsc = it.sc;
+    if (c.species) r.species = it.species;
     if (enter_tree(c, r)) {
       r.phase = kPhTree;
       return;
@@ -236,7 +249,7 @@ static __device__ __noinline__ bool ref_before_at(const float* __restrict__ Node
   return (na == left) == (lx < rx);
 }
 __device__ __forceinline__ bool ref_before(const TraceCtx& c, const Ray& r, int a, int b) {
-  return ref_before_at(c.Nodes, r.lro, r.linv, a, b);
+  return ref_before_at(scene_nodes(c, r.species), r.lro, r.linv, a, b);
 }
 
 // One interior step (Arbor.cu:224-225, 227).
@@ -247,8 +260,8 @@ __device__ __forceinline__ void tree_step(const TraceCtx& c, Ray& r, const Sibli
   }
   int left = r.node * 2;
   float4 llo, lhi, rlo, rhi;
-  load_node(c, left, llo, lhi);
-  load_node(c, left + 1, rlo, rhi);
+  load_node(c, r, left, llo, lhi);
+  load_node(c, r, left + 1, rlo, rhi);
   f2 ls, rs;
   bool lh = node_accept_span(llo, lhi, r.lro, r.linv, r.lbest, ls);
   bool rh = node_accept_span(rlo, rhi, r.lro, r.linv, r.lbest, rs);

@@ -42,6 +42,7 @@ struct WarpBatchQ {
   static constexpr int kWarpJobs = 32 * Q;
   float4 rayO[32];             // owner lane's local ray origin and wind time
   float4 rayD[32];             // owner lane's local ray direction
+  int rayS[32];                // owner lane's scene (forest of several species)
   LeafSolve solve[kNewtonCap];
   int prim[kWarpJobs];         // lane-major queue: lane * Q + k (leaf slot, then record id)
   float fp[kWarpJobs];
@@ -100,6 +101,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
   if (nq > 0) {
     b.rayO[lane] = make_float4(r.lro.x, r.lro.y, r.lro.z, r.ltime);
     b.rayD[lane] = make_float4(r.lrd.x, r.lrd.y, r.lrd.z, 0.0f);
+    if (c.species) b.rayS[lane] = r.species;
   }
   // Resolve each queued leaf slot to its record and test class: leaf clip,
   // wood (tube + SDF march, primary rays), the rest (stones, shadow-ray wood,
@@ -108,10 +110,10 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
   int nl = 0, nw = 0, nm = 0;
   for (int k = 0; k < nq; k++) {
     const int q = lane * WB::kQ + k;
-    const uint32_t uid = __ldg(c.Order + b.prim[q]);
+    const uint32_t uid = __ldg(scene_order(c, r.species) + b.prim[q]);
     int cls = kJobNone;
     if (uid < (uint32_t)kCapacity) {
-      const int t = (int)ldg4(c.P, (int)uid * 6).w;
+      const int t = (int)ldg4(scene_P(c, r.species), (int)uid * 6).w;
       cls = t == 1 ? kJobLeaf : (t == 0 && c.refine) ? kJobWood : kJobMisc;
     } else {
       b.res[q] = kFar;
@@ -161,7 +163,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
         int owner = q / WB::kQ;
         float4 o = b.rayO[owner], d = b.rayD[owner];
         float tube;
-        solve = leaf_clip(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls, tube);
+        solve = leaf_clip(scene_P(c, c.species ? b.rayS[owner] : 0), b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls, tube);
         b.res[q] = tube;  // the result, or the Newton stage's starting best
       }
       unsigned m = __ballot_sync(full, solve);
@@ -179,7 +181,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
     const int run = nN < 32 ? nN : 32;
     if (lane < run) {
       int qn = b.solveJob[lane];
-      b.res[qn] = leaf_newton(b.solve[lane], leaf_shape(c.P, b.prim[qn]), b.res[qn], b.fp[qn]);
+      b.res[qn] = leaf_newton(b.solve[lane], leaf_shape(scene_P(c, c.species ? b.rayS[qn / WB::kQ] : 0), b.prim[qn]), b.res[qn], b.fp[qn]);
     }
     __syncwarp();
     if (lane < nN - run) {
@@ -196,7 +198,7 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
       int q = b.job[totL + j];
       int owner = q / WB::kQ;
       float4 o = b.rayO[owner], d = b.rayD[owner];
-      b.res[q] = wood_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], true);
+      b.res[q] = wood_t(scene_P(c, c.species ? b.rayS[owner] : 0), b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], true);
     }
   }
   // stones, shadow-ray wood and unused records
@@ -206,7 +208,8 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
       int q = b.job[totL + totW + j];
       int owner = q / WB::kQ;
       float4 o = b.rayO[owner], d = b.rayD[owner];
-      b.res[q] = object_t(c.P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], o.w, c.wind, c.refine);
+      b.res[q] = object_t(scene_P(c, c.species ? b.rayS[owner] : 0), b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), b.fp[q], o.w, c.wind,
+                          c.refine);
     }
   }
   __syncwarp();

@@ -1,7 +1,7 @@
 """Benchmark: the 324-tree 1920x1080 forest walk (1 spp, sun shadows off).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl arbor|reference]
-                    [--workload forest|shadows|wind|tree|batch|denoise] [--no-cpu-baseline]
+                    [--workload forest|shadows|wind|tree|batch|denoise|species] [--no-cpu-baseline]
                     [--no-target]
 
 A step is one frame of the seeded 64-frame walk: updateCamera, tracePixels,
@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="arbor", choices=["arbor", "reference"])
-    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "wind", "tree", "batch", "denoise"])
+    ap.add_argument("--workload", default="forest", choices=["forest", "shadows", "wind", "tree", "batch", "denoise", "species"])
+    ap.add_argument("--species", type=int, default=16, help="species workload: distinct trees (scenes) in the forest")
     ap.add_argument("--views", type=int, default=64, help="batch workload: views per batch")
     ap.add_argument("--scenes", type=int, default=16, help="batch workload: resident scenes (master seeds)")
     ap.add_argument("--tune-views", type=int, default=8, help="batch workload: views the autotuner times each configuration on")
@@ -72,6 +73,10 @@ def workload_spec(name: str) -> dict:
         return {**base, "shadows": True,
                 "workload": "forest-1080p-walk-shadows: the forest walk with tree-to-tree sun shadows on "
                             "(sun elevation 35 deg, azimuth from the seed)"}
+    if name == "species":
+        return {**base, "species": 16,
+                "workload": "forest-1080p-walk-species: the forest walk (shadows off) with 16 species: instance t takes its own records and "
+                            "BVH from the scene of seed s[forestSeed(t, 7) mod 16] (seeds 7 and seeded draws), 16 scenes resident"}
     if name == "wind":
         return {**base, "shadows": True, "wind": True, "rebuild": True, "spp": 4,
                 "workload": "forest-1080p-wind: the forest walk at 4 spp per frame, sun shadows on (35 deg, azimuth from the seed), "
@@ -155,13 +160,30 @@ class Frames:
         self.w, self.h = w, h
         f32 = lambda n: torch.zeros(n, dtype=torch.float32, device="cuda")  # noqa: E731
         i32 = lambda n: torch.zeros(n, dtype=torch.int32, device="cuda")  # noqa: E731
-        self.B, self.P, self.Keys, self.Order, self.Nodes = f32(2109 * 20), f32(32768 * 24), i32(32768), i32(32768), f32(65536 * 8)
+        import workloads
+
+        ns = spec.get("species", 1)
+        self.B, self.P, self.Keys, self.Order, self.Nodes = (f32(2109 * 20), f32(ns * 32768 * 24), i32(ns * 32768), i32(ns * 32768),
+                                                             f32(ns * 65536 * 8))
         self.C = f32(64)
         self.scratch = i32(2 * 32768)
         self.Hit, self.Lin, self.Gui, self.Fil, self.Hist = (f32(w * h * 4) for _ in range(5))
         self.Pix = i32(w * h)
-        self.check(ab.call("arbor_buildScene", spec["seed"], self.B, self.P, self.Keys, self.Order, self.Nodes, self.C, self.scratch))
-        import workloads
+        self.species = None
+        if ns > 1:
+            # one scene per species seed, back to back; species 0 is the master seed
+            self.seeds = workloads.batch_seeds(ns, spec["seed"])
+            for k, sd in enumerate(self.seeds):
+                self.B.zero_()
+                sl = lambda t, n: t[k * n:(k + 1) * n]  # noqa: E731
+                self.check(ab.call("arbor_buildScene", sd, self.B, sl(self.P, 32768 * 24), sl(self.Keys, 32768), sl(self.Order, 32768),
+                                   sl(self.Nodes, 65536 * 8), self.C if k == 0 else None, self.scratch))
+            import ctypes
+
+            self.of = np.ascontiguousarray(workloads.species_of(ns, spec["seed"]), np.int32)
+            self.species = (ns, self.of.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        else:
+            self.check(ab.call("arbor_buildScene", spec["seed"], self.B, self.P, self.Keys, self.Order, self.Nodes, self.C, self.scratch))
 
         if spec["single_tree"]:
             self.C.copy_(torch.from_numpy(workloads.single_tree_camera(w, h, spec["seed"])))
@@ -185,10 +207,21 @@ class Frames:
         """The per-frame scene rebuild (camera record untouched)."""
         self.check(self.ab.call("arbor_buildScene", self.spec["seed"], self.B, self.P, self.Keys, self.Order, self.Nodes, None, self.scratch))
 
+    def trace_call(self):
+        if self.species:
+            return self.ab.call("arbor_traceSpeciesPixels", self.P, self.Nodes, self.Order, *self.species, self.C, self.Hit, self.w, self.h)
+        return self.ab.call(self.trace, self.P, self.Nodes, self.Order, self.C, self.Hit, self.w, self.h)
+
+    def shade_call(self):
+        if self.species:
+            return self.ab.call("arbor_shadeSpeciesPixels", self.P, self.Nodes, self.Order, *self.species, self.C, self.Hit, self.Lin, self.Gui,
+                                self.w, self.h)
+        return self.ab.call(self.shade, self.P, self.Nodes, self.Order, self.C, self.Hit, self.Lin, self.Gui, self.w, self.h)
+
     def sample(self):
         ab, w, h = self.ab, self.w, self.h
-        self.check(ab.call(self.trace, self.P, self.Nodes, self.Order, self.C, self.Hit, w, h))
-        self.check(ab.call(self.shade, self.P, self.Nodes, self.Order, self.C, self.Hit, self.Lin, self.Gui, w, h))
+        self.check(self.trace_call())
+        self.check(self.shade_call())
         self.check(ab.call("arbor_filterResolve", self.Lin, self.Gui, self.Hit, self.Fil, self.Hist, self.Pix, self.C, w, h))
 
     def step(self, k: int):
@@ -269,6 +302,8 @@ def run_arbor(args, rank: int, world: int, local_rank: int) -> None:
     spec = workload_spec(args.workload)
     if args.width and args.height:
         spec.update(width=args.width, height=args.height, workload=spec["workload"] + f" (at {args.width}x{args.height})")
+    if args.workload == "species":
+        spec["species"] = args.species
     result = measure_workload(args, spec, rank, world, local_rank)
     if args.workload == "forest" and not args.no_target:
         # The target configuration: the same walk with tree-to-tree sun
@@ -327,10 +362,10 @@ def measure_workload(args, spec: dict, rank: int, world: int, local_rank: int) -
     k0 = args.warmup + args.steps
     fr.step(k0)
     reps = 8
-    ms_trace = time_kernel(torch, lambda: fr.check(ab.call(fr.trace, fr.P, fr.Nodes, fr.Order, fr.C, fr.Hit, w, h)), reps)
-    ms_shade = time_kernel(torch, lambda: fr.check(ab.call(fr.shade, fr.P, fr.Nodes, fr.Order, fr.C, fr.Hit, fr.Lin, fr.Gui, w, h)), reps)
+    ms_trace = time_kernel(torch, lambda: fr.check(fr.trace_call()), reps)
+    ms_shade = time_kernel(torch, lambda: fr.check(fr.shade_call()), reps)
     ms_fr = time_kernel(torch, lambda: fr.check(ab.call("arbor_filterResolve", fr.Lin, fr.Gui, fr.Hit, fr.Fil, fr.Hist, fr.Pix, fr.C, w, h)), reps * 4)
-    ms_build = time_kernel(torch, fr.build, reps * 4)
+    ms_build = time_kernel(torch, fr.build, reps * 4) if not fr.species else None
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs")
     # filterLighting+resolvePixels algorithmic bytes per pixel: Linear, Guide,
@@ -350,18 +385,19 @@ def measure_workload(args, spec: dict, rank: int, world: int, local_rank: int) -
                    "l2": "per-step frame buffers (Hit, Linear, Guide, Filtered, History, Pixels = 174 MB at 1080p) exceed the "
                          "126 MB L2; the 5.7 MB scene stays resident by design"},
         "phases_ms": {"trace": round(ms_trace, 4), "shade": round(ms_shade, 4), "filter_resolve": round(ms_fr, 4),
-                      "build": round(ms_build, 4), "per_sample": ["trace", "shade", "filter_resolve"],
+                      "build": round(ms_build, 4) if ms_build else None, "per_sample": ["trace", "shade", "filter_resolve"],
                       "per_frame": (["build"] if spec["rebuild"] else []) + ["update_camera"] + (["set_sample"] if spec["spp"] > 1 else [])},
         "roofline": None,
         "roofline_hbm": {"kernel": "filterResolve", "bound": "hbm", "achieved": round(fr_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
                          "frac": round(fr_gbs / hbm_peak, 4) if hbm_peak else None, "traffic": None,
                          "algorithmic_bytes": fr_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
-        "roofline_build": {"kernel": "buildScene (growth, primitives + keys, 4 radix passes, bounds)", "bound": "hbm",
-                           "achieved": round(BUILD_BYTES / (ms_build / 1e3) / 1e9, 1), "peak": hbm_peak, "unit": "GB/s",
-                           "frac": round(BUILD_BYTES / (ms_build / 1e3) / 1e9 / hbm_peak, 4) if hbm_peak else None, "traffic": None,
-                           "algorithmic_bytes": BUILD_BYTES, "ms_per_build": round(ms_build, 4),
-                           "note": "13 MB over a few dependent launches of a few thousand threads: launch- and latency-bound, far "
-                                   "from the HBM roof", "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "roofline_build": None if not ms_build else {
+            "kernel": "buildScene (growth, primitives + keys, 4 radix passes, bounds)", "bound": "hbm",
+            "achieved": round(BUILD_BYTES / (ms_build / 1e3) / 1e9, 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(BUILD_BYTES / (ms_build / 1e3) / 1e9 / hbm_peak, 4) if hbm_peak else None, "traffic": None,
+            "algorithmic_bytes": BUILD_BYTES, "ms_per_build": round(ms_build, 4),
+            "note": "13 MB over a few dependent launches of a few thousand threads: launch- and latency-bound, far "
+                    "from the HBM roof", "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -369,20 +405,92 @@ def measure_workload(args, spec: dict, rank: int, world: int, local_rank: int) -
 
     # The FP32 roofline of the dominant kernel (trace, or shade when sun
     # shadows make it the longer pass); both are reported.
-    result["roofline_trace"] = roofline_model.trace_roofline(ab, fr, torch, ms_trace, fp32_peak, sm_clock)
-    result["roofline_shade"] = roofline_model.shade_roofline(ab, fr, torch, ms_shade, fp32_peak, sm_clock)
-    result["roofline"] = result["roofline_trace"] if ms_trace >= ms_shade else result["roofline_shade"]
+    if fr.species:
+        # the work counter runs one scene; no FP32 count for a forest of several species
+        result["roofline"] = result["roofline_hbm"]
+    else:
+        result["roofline_trace"] = roofline_model.trace_roofline(ab, fr, torch, ms_trace, fp32_peak, sm_clock)
+        result["roofline_shade"] = roofline_model.shade_roofline(ab, fr, torch, ms_shade, fp32_peak, sm_clock)
+        result["roofline"] = result["roofline_trace"] if ms_trace >= ms_shade else result["roofline_shade"]
 
     # End to end through the engine API with host buffers.
     if not args.no_e2e:
-        if spec["spp"] == 1 and not spec["rebuild"]:
+        if fr.species:
+            result["e2e"] = run_e2e_frames(ab, torch, fr, args)
+        elif spec["spp"] == 1 and not spec["rebuild"]:
             result["e2e"] = run_e2e(ab, torch, spec, args)
         else:
             result["e2e"] = {"value": None, "unit": UNIT, "note": "the engine API renders one sample per frame without rebuilds"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(spec, args.cpu_seconds)
+        result["cpu_baseline"] = cpu_species_sample(fr, args.cpu_seconds) if fr.species else cpu_baseline(spec, args.cpu_seconds)
     del fr
     return result
+
+
+def run_e2e_frames(ab, torch, fr, args) -> dict:
+    """End to end through the C-ABI entries: every step copies the frame's
+    input record from pinned host memory, runs the frame and copies the
+    RGBA8 frame back to pinned host memory."""
+    import workloads
+
+    w, h = fr.w, fr.h
+    stream = torch.cuda.current_stream()
+    inputs = torch.from_numpy(np.stack([workloads.walk_input(k, fr.spec["seed"])[0] for k in range(WALK_FRAMES)])).pin_memory()
+    I_dev = torch.zeros(32, device="cuda")
+    host = torch.empty(w * h, dtype=torch.int32).pin_memory()
+
+    def one(k):
+        I_dev.copy_(inputs[k % WALK_FRAMES], non_blocking=True)
+        fr.check(ab.call("arbor_updateCamera", fr.C, I_dev, fr.P, fr.dts[k % WALK_FRAMES], w, h))
+        fr.sample()
+        host.copy_(fr.Pix, non_blocking=True)
+
+    for k in range(args.warmup):
+        one(k)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for k in range(args.steps):
+        one(args.warmup + k)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    return {"value": round(w * h * args.steps / (ms / 1e3) / 1e6, 3), "unit": UNIT, "h2d_bytes_per_step": 32 * 4,
+            "d2h_bytes_per_step": w * h * 4, "ms_per_step": round(ms / args.steps, 4),
+            "api": "arbor_updateCamera + arbor_traceSpeciesPixels + arbor_shadeSpeciesPixels + arbor_filterResolve (pinned host buffers)"}
+
+
+def cpu_species_sample(fr, target_s: float) -> dict:
+    """The oracle's forest of several species (each instance's traceTree on
+    its own scene, as the reference composes traceTree per instance) on a
+    band of rows of the walk's first frame."""
+    o, _ = cpu_oracle()
+    if not hasattr(o.lib, "oracle_tracePixelsSpecies"):
+        from pyoracle import Oracle
+
+        o = Oracle("port")
+    import workloads
+
+    spec = fr.spec
+    w, h = spec["width"], spec["height"]
+    scenes = [o.build_scene(sd) for sd in fr.seeds]
+    C = workload_state(o.init_camera(scenes[0]["P"], spec["seed"]), spec)
+    I, dt = workloads.walk_input(0, spec["seed"])
+    o.update_camera(C, I, scenes[0]["P"], dt, w, h)
+    rows = max(4, o.max_threads())
+    y0 = h // 2 - rows // 2
+    for _ in range(2):
+        t0 = time.perf_counter()
+        hit = o.trace_species(scenes, fr.of, C, w, h, y0, y0 + rows)
+        o.shade_species(scenes, fr.of, C, hit, w, h, y0, y0 + rows)
+        secs = time.perf_counter() - t0
+        if secs >= target_s * 0.5 or rows >= h // 2:
+            break
+        rows = int(min(h // 2, max(rows, rows * target_s / max(secs, 1e-3))))
+        y0 = h // 2 - rows // 2
+    return {"value": round(rows * w / secs / 1e6, 4), "unit": UNIT, "cores": o.max_threads(), "kind": "port",
+            "sample": f"rows {y0}..{y0 + rows - 1} of frame 0 ({rows * w} primary rays, {secs:.2f} s): trace and shade of the "
+                      "oracle's forest of several species (the reference has no such forest)", "seconds": round(secs, 3)}
 
 
 def run_e2e(ab, torch, spec: dict, args) -> dict:
@@ -504,6 +612,9 @@ def run_reference(args, rank: int) -> None:
     if args.workload == "batch":
         run_reference_batch(args)
         return
+    if args.workload == "species":
+        run_reference_species(args)
+        return
     spec = workload_spec(args.workload)
     if args.width and args.height:
         spec.update(width=args.width, height=args.height)
@@ -526,6 +637,28 @@ def run_reference(args, rank: int) -> None:
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": o.max_threads(), "kind": kind,
                              "sample": f"each step renders {n} evenly strided rows of {spec['height']} of frame 0 "
                                        f"({rays} primary rays): trace, shade, filter, resolve"},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_species(args) -> None:
+    """The oracle's forest of several species (no reference counterpart) on
+    a band of rows per step, on all host cores."""
+    import types
+
+    import workloads
+
+    spec = workload_spec("species")
+    ns = args.species
+    spec["species"] = ns
+    fr = types.SimpleNamespace(spec=spec, seeds=workloads.batch_seeds(ns, spec["seed"]), of=workloads.species_of(ns, spec["seed"]))
+    step_s = float(os.environ.get("ARBOR_REFERENCE_STEP_SECONDS", "2.0"))
+    samples = [cpu_species_sample(fr, step_s) for _ in range(args.warmup + args.steps)][args.warmup:]
+    value = statistics.mean(x["value"] for x in samples)
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * statistics.mean(x["seconds"] for x in samples), 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic: procedural scenes grown from the species seeds", "impl": "reference",
+            "config": spec, "cpu_baseline": {k: samples[-1][k] for k in ("unit", "cores", "kind", "sample")} | {"value": round(value, 4)},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -202,6 +202,22 @@ ARBOR_API int arbor_shadeTreePixels(const float* P, const float* Nodes, const ui
 ARBOR_API int arbor_tracePixelsInOrder(const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width, int height, int single_tree, arbor_stream stream);
 ARBOR_API int arbor_shadePixelsInOrder(const float* P, const float* Nodes, const uint32_t* Order, const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, int single_tree, arbor_stream stream);
 
+/* A forest of several species (no reference counterpart: the reference's
+ * 324 instances all share one resident tree, README.md:8,
+ * docs/ARCHITECTURE.md:5).  Instance t keeps the reference's transform, wind
+ * phase and tint (forestPos/Scale/Yaw/Seed of t, Arbor.cu:57-69) but takes
+ * its geometry - its own records and its own BVH - from scene species_of[t]
+ * (host array of ARBOR_FOREST_COUNT ints in 0..n_species-1).  P, Nodes and
+ * Order hold n_species scenes back to back (each the ABI size: 32768*24,
+ * 65536*8 and 32768 elements), e.g. n_species arbor_buildScene results with
+ * different seeds.  Hit.primId is a record id of the hit instance's scene.
+ * The 2D DDA and bounding spheres are the reference's.  With every
+ * species_of[t] = 0 the results equal arbor_tracePixels / arbor_shadePixels
+ * on scene 0.  n_species at most ARBOR_MAX_SPECIES. */
+#define ARBOR_MAX_SPECIES 256
+ARBOR_API int arbor_traceSpeciesPixels(const float* P, const float* Nodes, const uint32_t* Order, int n_species, const int* species_of, const float* C, float* Hit, int width, int height, arbor_stream stream);
+ARBOR_API int arbor_shadeSpeciesPixels(const float* P, const float* Nodes, const uint32_t* Order, int n_species, const int* species_of, const float* C, const float* Hit, float* Linear, float* Guide, int width, int height, arbor_stream stream);
+
 /* shadePixels (Arbor.cu:277-289) that also writes the shading normal of
  * each pixel (world space, facing the camera; zero for sky) into Normal
  * (W*H float4, .w = 0): the G-buffer the learned denoiser reads.  No
