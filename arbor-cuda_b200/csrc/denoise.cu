@@ -6,7 +6,9 @@
 //
 // Arithmetic: activations and weights in BF16, tensor-core products
 // accumulated in FP32 (tcgen05.mma with TMEM accumulators for the forward
-// convolutions; mma.sync m16n8k16 for the backward passes), FP32 master
+// convolutions and the backward data pass, except the data pass of the two
+// widest decoder inputs (160 and 224 channels) and the weight gradients,
+// which use mma.sync m16n8k16), FP32 master
 // weights, biases, gradients and Adam moments.  Activations are NHWC with channel counts that
 // are multiples of 16.
 //
@@ -21,7 +23,9 @@
 //                   data pass on rotated, transposed weights, with the
 //                   previous layer's activation derivative in its epilogue.
 //   wgrad_kernel    weight gradients: a GEMM over pixels of the output
-//                   gradient and the shifted input, FP32 atomics per CTA
+//                   gradient and the shifted input; each CTA writes its
+//                   pixel range's partial sums, reduce_kernel adds the
+//                   partials in a fixed order (deterministic gradients)
 //   pool / upcat    2x2 average pooling and its backward pass; the backward
 //                   pass of nearest upsampling + skip concatenation (the
 //                   forward concatenation is read in place by the decoder
@@ -484,6 +488,7 @@ __global__ void __launch_bounds__(128) conv_row_kernel(ConvArgs a, int rows_per_
         for (int j = 0; j < 16; j++) {
           float x = __uint_as_float(v[j]) + bias_s[col + j];
           if (a.act) x = x > 0.0f ? x : x * kSlope;
+          if (a.mask && !(__bfloat162float(a.mask[p * a.cout + col + j]) > 0.0f)) x *= kSlope;
           f[j] = x;
         }
         if (a.y_fp32) {
@@ -552,7 +557,7 @@ __global__ void __launch_bounds__(128) conv_row_kernel(ConvArgs a, int rows_per_
 struct WgradArgs {
   const bf16* dy;  // NHWC, cout channels
   const bf16* x;   // NHWC, cin channels (or cs channels with x2, as ConvArgs)
-  float* dw;       // [cout][9][cin], accumulated
+  float* dw;       // partial sums: [gridDim.x][cout][9][cin], one slice per pixel range
   int cin, cout, n, h, w;
   int pixels_per_cta;
   const bf16* x2;
@@ -627,14 +632,14 @@ __global__ void __launch_bounds__(128) wgrad_kernel(WgradArgs a) {
       const int co = co0 + warp * 16 + g + 8 * hh;
       if (co >= a.cout) continue;
       const int ci = ci0 + nt * 8 + 2 * t;
-      float* d = a.dw + ((size_t)co * 9 + tap) * a.cin + ci;
-      atomicAdd(d, acc[nt][2 * hh]);
-      atomicAdd(d + 1, acc[nt][2 * hh + 1]);
+      float* d = a.dw + (size_t)blockIdx.x * a.cout * 9 * a.cin + ((size_t)co * 9 + tap) * a.cin + ci;
+      d[0] = acc[nt][2 * hh];
+      d[1] = acc[nt][2 * hh + 1];
     }
   }
 }
 
-// db[co] += sum over pixels of dY[p][co]
+// Partial bias gradients: db[blockIdx.x][co] = sum over this block's pixels of dY[p][co]
 __global__ void bgrad_kernel(const bf16* __restrict__ dy, float* __restrict__ db, int cout, long pixels) {
   __shared__ float part[256];
   const int tid = threadIdx.x;
@@ -650,7 +655,17 @@ __global__ void bgrad_kernel(const bf16* __restrict__ dy, float* __restrict__ db
   if (tid < cout) {
     float t = 0.0f;
     for (int k = tid; k < lanes; k += cout) t += part[k];
-    atomicAdd(db + tid, t);
+    db[(size_t)blockIdx.x * cout + tid] = t;
+  }
+}
+
+// g[i] += sum over s = 0 .. splits - 1, in that order, of part[s * n + i]:
+// the partial sums of wgrad_kernel / bgrad_kernel folded in a fixed order.
+__global__ void reduce_kernel(const float* __restrict__ part, float* __restrict__ g, long n, int splits) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int k = 0; k < splits; k++) s += part[(size_t)k * n + i];
+    g[i] += s;
   }
 }
 
@@ -948,6 +963,8 @@ struct arbor_denoiser {
   float* loss = nullptr;  // device scalar
   float loss_host = 0.0f;
   int* err = nullptr;     // device flag: a tcgen05 wait gave up
+  float* part = nullptr;  // partial weight / bias gradients of one layer (wgrad_kernel, bgrad_kernel)
+  size_t part_floats = 0;
   bool tc = true;         // forward convolutions on tcgen05
   long steps = 0;
   size_t allocated = 0;
@@ -1061,9 +1078,9 @@ int launch_conv_tc(const ConvArgs& a, int* err, cudaStream_t s) {
   }
 }
 
-int launch_wgrad(const bf16* dy, const bf16* x, const bf16* x2, int cs, float* dw, int cin, int cout, int n, int h, int w, cudaStream_t s) {
-  WgradArgs a{dy, x, dw, cin, cout, n, h, w, 0, x2, cs};
-  const long pixels = (long)n * h * w;
+// Pixel ranges of one layer's weight-gradient GEMM: about 1184 CTAs (8 per
+// SM) over (cout / 64) x 9 x (cin / ci_tile) tiles, ranges of >= 256 pixels.
+long wgrad_per(long pixels, int cin, int cout) {
   const int ci_tile = cin % 32 == 0 ? 32 : 16;
   const int base = ((cout + 63) / 64) * 9 * (cin / ci_tile);
   long split = 1184 / base;
@@ -1071,13 +1088,38 @@ int launch_wgrad(const bf16* dy, const bf16* x, const bf16* x2, int cs, float* d
   long per = (pixels + split - 1) / split;
   per = (per + 31) / 32 * 32;
   if (per < 256) per = 256;
+  return per;
+}
+// Largest number of pixel ranges wgrad_per gives for any pixel count.
+long wgrad_max_splits(int cin, int cout) {
+  const int ci_tile = cin % 32 == 0 ? 32 : 16;
+  const long base = ((cout + 63) / 64) * 9 * (cin / ci_tile);
+  return std::max(1L, 1184 / base) + 1;
+}
+constexpr int kBgradBlocks = 1184;
+
+// dw += the layer's weight gradient: partial sums per pixel range into
+// `part`, then folded in range order (the same sums whatever the schedule).
+int launch_wgrad(const bf16* dy, const bf16* x, const bf16* x2, int cs, float* dw, float* part, size_t part_floats, int cin, int cout, int n,
+                 int h, int w, cudaStream_t s) {
+  WgradArgs a{dy, x, part, cin, cout, n, h, w, 0, x2, cs};
+  const long pixels = (long)n * h * w;
+  const int ci_tile = cin % 32 == 0 ? 32 : 16;
+  const long per = wgrad_per(pixels, cin, cout);
   a.pixels_per_cta = (int)per;
-  const dim3 grid((unsigned)((pixels + per - 1) / per), (unsigned)((cout + 63) / 64), (unsigned)(9 * (cin / ci_tile)));
+  const long splits = (pixels + per - 1) / per;
+  const long size = (long)cout * 9 * cin;
+  if ((size_t)(splits * size) > part_floats) {
+    set_error("launch_wgrad: %ld partial gradients exceed the %zu-float buffer", splits * size, part_floats);
+    return ARBOR_ERR_LIMIT;
+  }
+  const dim3 grid((unsigned)splits, (unsigned)((cout + 63) / 64), (unsigned)(9 * (cin / ci_tile)));
   if (ci_tile == 32)
     wgrad_kernel<32><<<grid, 128, 0, s>>>(a);
   else
     wgrad_kernel<16><<<grid, 128, 0, s>>>(a);
-  count_launch();
+  reduce_kernel<<<ew_grid(size), 256, 0, s>>>(part, dw, size, (int)splits);
+  count_launch(2);
   return check_launch("wgrad_kernel");
 }
 
@@ -1148,11 +1190,13 @@ int backward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
     const int lv = kAct[kIn[l]].level;
     const bool cat = kCat[l][0] >= 0;
     if (int st = launch_wgrad(dy, cat ? d->act[kCat[l][0]] : x_of(l), cat ? d->act[kCat[l][1]] : nullptr, cat ? kAct[kCat[l][0]].channels : 0,
-                              d->g + L.woff, L.cin, L.cout, batch, h >> lv, w >> lv, s))
+                              d->g + L.woff, d->part, d->part_floats, L.cin, L.cout, batch, h >> lv, w >> lv, s))
       return st;
     const long px = level_pixels(d, lv, batch, w, h);
-    bgrad_kernel<<<(unsigned)std::min<long>(1184, (px * L.cout + 255) / 256 + 1), 256, 0, s>>>(dy, d->g + L.boff, L.cout, px);
-    count_launch();
+    const unsigned blocks = (unsigned)std::min<long>(kBgradBlocks, (px * L.cout + 255) / 256 + 1);
+    bgrad_kernel<<<blocks, 256, 0, s>>>(dy, d->part, L.cout, px);
+    reduce_kernel<<<1, 256, 0, s>>>(d->part, d->g + L.boff, L.cout, (int)blocks);
+    count_launch(2);
     return check_launch("bgrad_kernel");
   };
   // input gradient of layer l: conv of dY with the rotated, transposed
@@ -1162,7 +1206,10 @@ int backward(arbor_denoiser* d, const bf16* features, int batch, int w, int h) {
     const int lv = kAct[kIn[l]].level;
     ConvArgs a{dy, d->wb + d->wf_off[l], nullptr, dx, mask_act >= 0 ? d->act[mask_act] : nullptr, L.cout, L.cin, batch, h >> lv, w >> lv, 0, 0,
                nullptr, 0};
-    return launch_conv(a, s);
+    // tcgen05 where the output width has a tensor-core kernel (all but the
+    // 160- and 224-channel decoder inputs); the same K = 16 accumulation order
+    // as the mma.sync kernel.
+    return d->tc && tc_shape(a) ? launch_conv_tc(a, d->err, s) : launch_conv(a, s);
   };
   auto upcat_back = [&](int cat, int skip_level, int low) {
     const int lv = kAct[cat].level;
@@ -1292,6 +1339,12 @@ extern "C" int arbor_denoiser_create(arbor_denoiser** out, int max_batch, int ma
       return fail(cuda_fail("cudaMalloc (denoiser concat gradients)", ce));
   if (!alloc((void**)&d->out, (size_t)px0 * kOutC * 4) || !alloc((void**)&d->dout, (size_t)px0 * kOutC * 2))
     return fail(cuda_fail("cudaMalloc (denoiser output)", ce));
+  for (int l = 0; l < kLayers; l++) {
+    const LayerParams& L = d->layer[l];
+    d->part_floats = std::max(d->part_floats, (size_t)(wgrad_max_splits(L.cin, L.cout) * L.cout * 9 * L.cin));
+    d->part_floats = std::max(d->part_floats, (size_t)kBgradBlocks * L.cout);
+  }
+  if (!alloc((void**)&d->part, d->part_floats * 4)) return fail(cuda_fail("cudaMalloc (denoiser partial gradients)", ce));
   // He-normal weights (the output layer 10x smaller), zero biases and moments
   if ((ce = cudaMemsetAsync(d->err, 0, 4, stream)) != cudaSuccess || (ce = cudaMemsetAsync(d->p, 0, pb, stream)) != cudaSuccess ||
       (ce = cudaMemsetAsync(d->g, 0, pb, stream)) != cudaSuccess ||
@@ -1480,7 +1533,7 @@ extern "C" int arbor_denoiser_check(arbor_denoiser* d) {
 extern "C" int arbor_denoiser_destroy(arbor_denoiser* d) {
   if (d == nullptr) return ARBOR_OK;
   if (d->stream) cudaStreamSynchronize(d->stream);
-  void* bufs[] = {d->p, d->g, d->m, d->v, d->wf, d->wb, d->out, d->dout, d->loss, d->err, d->dcat[0], d->dcat[1], d->dcat[2]};
+  void* bufs[] = {d->p, d->g, d->m, d->v, d->wf, d->wb, d->out, d->dout, d->loss, d->err, d->part, d->dcat[0], d->dcat[1], d->dcat[2]};
   for (void* p : bufs)
     if (p) cudaFree(p);
   for (int k = 0; k < kActs; k++) {

@@ -294,3 +294,70 @@ def test_tcgen05_forward_matches_mma_sync(cuda, w, h):
         assert rms <= 5e-4 * max(1.0, scale)
     finally:
         net.close()
+
+
+def train(net, feat, noisy, target, steps, lr=2e-3, batch=2, w=32, h=32):
+    f, n, t = to_dev_bf16(feat), noisy.contiguous().cuda(), target.contiguous().cuda()
+    for _ in range(steps):
+        assert net.lib.arbor_denoiser_train_step(net.h, f.data_ptr(), n.data_ptr(), t.data_ptr(), batch, w, h, lr, None) == ab.OK, \
+            ab.last_error()
+    return net.params()
+
+
+def test_training_is_deterministic_and_gradient_leaves_no_state(cuda):
+    """Weight and bias gradients are folded in a fixed order (no atomics), so
+    training is reproducible bit for bit; and arbor_denoiser_gradient leaves
+    the parameters, the Adam moments and the gradient accumulator as it found
+    them: gradient() then three train steps gives exactly the parameters of
+    three train steps alone."""
+    batch, w, h = 2, 32, 32
+    feat, noisy, target = random_inputs(batch, w, h, seed=6)
+    a, b = Net(batch, w, h, seed=8), Net(batch, w, h, seed=8)
+    try:
+        grad = np.zeros(a.count, np.float32)
+        f, n, t = to_dev_bf16(feat), noisy.contiguous().cuda(), target.contiguous().cuda()
+        assert a.lib.arbor_denoiser_gradient(a.h, f.data_ptr(), n.data_ptr(), t.data_ptr(), batch, w, h, grad.ctypes.data, grad.size,
+                                             None) == ab.OK, ab.last_error()
+        g2 = np.zeros(a.count, np.float32)
+        assert a.lib.arbor_denoiser_gradient(a.h, f.data_ptr(), n.data_ptr(), t.data_ptr(), batch, w, h, g2.ctypes.data, g2.size,
+                                             None) == ab.OK
+        assert np.array_equal(grad, g2), "the same gradient twice"
+        pa = train(a, feat, noisy, target, 3)
+        pb = train(b, feat, noisy, target, 3)
+        print(f"[denoiser determinism] parameters differ at {int((pa != pb).sum())} of {pa.numel()}")
+        assert torch.equal(pa, pb)
+    finally:
+        a.close()
+        b.close()
+
+
+def test_backward_data_pass_on_tcgen05_matches_mma_sync(cuda):
+    """The gradient with the forward and backward data convolutions on
+    tcgen05 against the same gradient with every convolution on mma.sync:
+    both accumulate the same K = 16 products in the same order; the bar
+    allows neighbouring BF16 roundings of the stored activations and
+    gradients (relative L2 difference <= 1e-2 per layer)."""
+    batch, w, h = 2, 64, 32
+    feat, noisy, target = random_inputs(batch, w, h, seed=7)
+    net = Net(batch, w, h, seed=10)
+    try:
+        f, n, t = to_dev_bf16(feat), noisy.contiguous().cuda(), target.contiguous().cuda()
+        grads = {}
+        for tc in (1, 0):
+            assert net.lib.arbor_denoiser_set_backend(net.h, tc) == ab.OK
+            g = np.zeros(net.count, np.float32)
+            assert net.lib.arbor_denoiser_gradient(net.h, f.data_ptr(), n.data_ptr(), t.data_ptr(), batch, w, h, g.ctypes.data, g.size,
+                                                   None) == ab.OK, ab.last_error()
+            assert net.lib.arbor_denoiser_check(net.h) == ab.OK, ab.last_error()
+            grads[tc] = torch.from_numpy(g).double()
+        off, worst = 0, 0.0
+        for cin, cout, _ in SPEC:
+            k = cout * 9 * cin + cout
+            a_, b_ = grads[1][off:off + k], grads[0][off:off + k]
+            worst = max(worst, float((a_ - b_).norm() / (b_.norm() + 1e-30)))
+            off += k
+        exact = int((grads[1] == grads[0]).sum())
+        print(f"[denoiser backward tcgen05 vs mma.sync] worst layer relative difference {worst:.3g}; {exact} of {net.count} equal")
+        assert worst <= 1e-2
+    finally:
+        net.close()
