@@ -99,6 +99,10 @@ __device__ __forceinline__ Wood load_wood(const float* P, int id) {
 }
 // Voronoi bark relief (Arbor.cu:149-169).  fine/grain are the footprint
 // band weights of the 10 mm and 2.5 mm bands (constant per call).
+// kMarch: the SDF march of the intersection test, whose angular terms take
+// the hardware sine/cosine (below); shading and normals (kMarch false) keep
+// the accurate functions.
+template <bool kMarch = false>
 __device__ __forceinline__ float bark_cut(const Wood& w, f3 p, float fp, float fine, float grain) {
   f3 pa = p - w.a;
   float along = sat(dot3(pa, w.ab) / fmaxf(0.000001f, w.abab));
@@ -111,9 +115,24 @@ __device__ __forceinline__ float bark_cut(const Wood& w, f3 p, float fp, float f
   float z = dot3(pa, w.d);
   float theta = atan2f(dot3(pa, w.v), dot3(pa, w.u));
   float arc = w.arc0 + z;
-  float st = sinf(theta), ct = cosf(theta);
-  float x = (theta / (2.0f * kPi) + 0.5f) * (float)w.columns + 0.32f * sinf(arc * 6.7f + ct * 3.0f) + 0.15f * sinf(arc * 19.0f + st * 2.0f);
-  float y = arc / 0.19f + 0.25f * sinf(theta * 7.0f) + 0.1f * sinf(theta * 19.0f);
+  // In the march the relief's angular terms use the hardware sine/cosine
+  // (absolute error about 2^-21 per unit of argument magnitude: below 1e-4
+  // for the arguments here, |x| < 700): they shift the Voronoi plates by far
+  // less than a footprint, and the relief enters the SDF scaled by
+  // amp <= 0.021.  The whole-frame IDs and distances stay within the
+  // contract (tests pin them).
+  float st, ct, x, y;
+  if (kMarch) {
+    st = __sinf(theta);
+    ct = __cosf(theta);
+    x = (theta / (2.0f * kPi) + 0.5f) * (float)w.columns + 0.32f * __sinf(arc * 6.7f + ct * 3.0f) + 0.15f * __sinf(arc * 19.0f + st * 2.0f);
+    y = arc / 0.19f + 0.25f * __sinf(theta * 7.0f) + 0.1f * __sinf(theta * 19.0f);
+  } else {
+    st = sinf(theta);
+    ct = cosf(theta);
+    x = (theta / (2.0f * kPi) + 0.5f) * (float)w.columns + 0.32f * sinf(arc * 6.7f + ct * 3.0f) + 0.15f * sinf(arc * 19.0f + st * 2.0f);
+    y = arc / 0.19f + 0.25f * sinf(theta * 7.0f) + 0.1f * sinf(theta * 19.0f);
+  }
   int ix = (int)floorf(x);
   int iy = (int)floorf(y);
   int wrapped[3];
@@ -149,10 +168,11 @@ __device__ __forceinline__ float bark_cut(const Wood& w, f3 p, float fp, float f
   return amp * clampf(0.32f + coarse * (plates - 0.37f) * 0.69f + fine * (splinter - 0.5f) * 0.24f + grain * (pores - 0.5f) * 0.08f, 0.005f, 1.0f);
 }
 // Wood SDF (Arbor.cu:170).
+template <bool kMarch = false>
 __device__ __forceinline__ float wood_field(const Wood& w, f3 p, float fp, float fine, float grain) {
   float t = sat(dot3(p - w.a, w.ab) / fmaxf(0.0000001f, w.abab));
   float radius = lerpf(w.ra, w.rb, t);
-  return length3(p - w.a - w.ab * t) - radius + bark_cut(w, p, fp, fine, grain);
+  return length3(p - w.a - w.ab * t) - radius + bark_cut<kMarch>(w, p, fp, fine, grain);
 }
 
 // --------------------------------------------------------------- leaf --
@@ -211,7 +231,11 @@ __device__ __forceinline__ float leaf_height(float u, float v, float len, float 
 // leaf_height in parts, for the Newton stage's five evaluations at
 // (u, v), (u +- e, v), (u, v +- e): the along-blade terms of one u and the
 // across-blade terms of one v are each computed once and shared.  Each
-// height is assembled with exactly leaf_height's operations.
+// height is assembled with exactly leaf_height's operations.  The iterations
+// take the hardware sine and exponential (absolute errors near 1e-6 for these
+// arguments, |x| < 4, against a height scale of centimetres); they only steer
+// the iterate - the acceptance test at the end (leaf_height, leaf_width)
+// evaluates the accurate functions.
 struct LeafU {
   float q, s;
 };
@@ -220,9 +244,9 @@ struct LeafV {
 };
 __device__ __forceinline__ LeafU leaf_u(float u, float len) {
   const float q = clampf(u / len, -0.2f, 1.2f);
-  return {q, sinf(kPi * q)};
+  return {q, __sinf(kPi * q)};
 }
-__device__ __forceinline__ LeafV leaf_v(float v, float hw2) { return {v * v / hw2, expf(-fabsf(v) / 0.005f)}; }
+__device__ __forceinline__ LeafV leaf_v(float v, float hw2) { return {v * v / hw2, __expf(-fabsf(v) / 0.005f)}; }
 __device__ __forceinline__ float leaf_height_parts(const LeafU& a, float v, const LeafV& b, float curl, float twist, float bw007) {
   float coarse = curl * a.s + twist * (a.q - 0.4f) * v + 0.009f * b.vv * a.s;
   float mid = 0.0012f * b.ev * a.s * bw007;
@@ -296,7 +320,7 @@ static __device__ __noinline__ float wood_t(const float* P, int id, f3 ro, f3 rd
   float grain = band_weight(0.0025f, footprint);
   for (int k = 0; k < 64; k++) {
     ARBOR_COUNT(kEvMarch);
-    float f = wood_field(w, ro + rd * t, footprint, fine, grain);
+    float f = wood_field<true>(w, ro + rd * t, footprint, fine, grain);
     if (f < eps) return t;
     t += fmaxf(eps * 0.35f, f * 0.27f);
     if (t > span.y) return kFar;

@@ -498,6 +498,22 @@ constexpr int kSX = kFX + 2 * kHalo, kSY = kFY + 2 * kHalo;
 // Arbor.cu:303
 __device__ __forceinline__ float aces(float x) { return sat((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f)); }
 
+// The filter and resolve keep the transcendental / conversion unit (which
+// runs divisions' reciprocals, exp2/log2 and int<->float conversions at an
+// eighth of the FMA rate) for the IEEE divisions the reference's results
+// need; truncations and floors of small values are taken in FP32 adds with
+// directed rounding instead: for |v| < 2^22, v + 1.5 * 2^23 lies in
+// [2^23, 2^24), where consecutive floats are consecutive integers, so the
+// sum rounded toward zero / toward minus infinity is 1.5 * 2^23 + trunc(v) /
+// + floor(v) exactly, and the integer difference of the bit patterns is that
+// integer.
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr int kMagicBits = 0x4B400000;
+
+// Vignette coordinate of column x of a width-pixel image (row y of a height
+// one): ((float)x / (float)width - 0.5) * 2 (Arbor.cu:304).
+__device__ __forceinline__ float vig_coord(int x, int width) { return ((float)x / (float)width - 0.5f) * 2.0f; }
+
 // One channel of resolvePixels' output byte (Arbor.cu:304, packRGB :49):
 // byte = (uint)(t), t = sat(pow(aces(c), 1/2.2) * vig) * 255 + 0.5, with the
 // power taken as the float of the double-precision pow (xpow) and aces with
@@ -507,31 +523,34 @@ __device__ __forceinline__ float aces(float x) { return sat((x * (2.51f * x + 0.
 // the power is above 1e-3, and an absolute error below 1e-9 under it), so its
 // t is within 3e-4 of the exact t; where it lies within 1e-3 of an integer
 // the exact t decides.  Same bytes as the exact evaluation, far fewer
-// instructions.
+// instructions.  t lies in [0.5, 255.5], so its floor is taken with kMagic.
 __device__ __forceinline__ uint32_t gamma_byte(float c, float vig) {
   const float a = sat(__fdividef(c * (2.51f * c + 0.03f), c * (2.43f * c + 0.59f) + 0.14f));
   float t = sat(__powf(a, 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
-  const float fr = t - floorf(t);
+  float fl = __fadd_rd(t, kMagic);  // kMagic + floor(t)
+  const float fr = t - (fl - kMagic);
   // (|c| >= 1e18 also takes the exact path: there the approximate division's
   // denominator can pass 2^126, where __fdividef returns 0.)
-  if (fr < 1e-3f || fr > 1.0f - 1e-3f || !(fabsf(c) < 1e18f)) t = sat(xpow(aces(c), 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
-  return (uint32_t)t;
+  if (fr < 1e-3f || fr > 1.0f - 1e-3f || !(fabsf(c) < 1e18f)) {
+    t = sat(xpow(aces(c), 1.0f / 2.2f) * vig) * 255.0f + 0.5f;
+    fl = __fadd_rd(t, kMagic);
+  }
+  return (uint32_t)(__float_as_int(fl) - kMagicBits);
 }
 
-// Arbor.cu:304, one pixel: `current` is the filtered colour.
-__device__ __forceinline__ void resolve_px(f3 current, float* __restrict__ History, uint32_t* __restrict__ Pixels, float c9, float c10,
-                                           float exposure, int x, int y, int width, int height) {
-  int i = y * width + x;
-  float count = c10 > 0.5f ? 0.0f : c9;
+// Arbor.cu:304, one pixel i: `current` is the filtered colour; count is the
+// sample count (C[10] > 0.5 ? 0 : C[9]) and inv = 1 / (count + 1), the same
+// for every pixel; u, v the pixel's vignette coordinates (vig_coord).
+__device__ __forceinline__ void resolve_px(f3 current, float* __restrict__ History, uint32_t* __restrict__ Pixels, float count, float inv,
+                                           float exposure, float u, float v, int i) {
   f3 mean = current;
-  if (!(count < 0.5f)) mean = mix3(xyz(reinterpret_cast<const float4*>(History)[i]), current, 1.0f / (count + 1.0f));
+  if (!(count < 0.5f)) mean = mix3(xyz(reinterpret_cast<const float4*>(History)[i]), current, inv);
   reinterpret_cast<float4*>(History)[i] = make_float4(mean.x, mean.y, mean.z, count + 1.0f);
   const f3 col = mean * exposure;
-  float u = ((float)x / (float)width - 0.5f) * 2.0f;
-  float v = ((float)y / (float)height - 0.5f) * 2.0f;
   const float vig = 1.0f - 0.09f * (u * u + v * v);
   Pixels[i] = gamma_byte(col.x, vig) | (gamma_byte(col.y, vig) << 8) | (gamma_byte(col.z, vig) << 16) | 4278190080u;
 }
+__device__ __forceinline__ float sample_count(float c9, float c10) { return c10 > 0.5f ? 0.0f : c9; }
 
 // Same-surface 5x5 demodulated filter (Arbor.cu:292-302) of one kFX x kFY
 // tile, staged with a 2-pixel halo in shared memory so each input pixel is
@@ -552,6 +571,7 @@ struct FilterTile {
   int2 key[kSY][kSX];      // depth bits, packed surface key
   float4 demod[kSY][kSX];  // Linear / (Guide + 0.02)
   float w[6];              // weights of r^2 = 0, 1, 2, 4, 5, 8
+  float u[kFX], v[kFY];    // vignette coordinates of the tile's columns and rows
 };
 
 // Weight of tap (j, k), from the staged exp(-0.3 r^2) values (compile-time index).
@@ -631,45 +651,99 @@ __device__ __noinline__ f3 filter_px_direct(const float* __restrict__ Linear, co
   return col;
 }
 
-// Packed surface key of a Hit record, or -1 (never a packed key) when its
-// ids lie outside -1..65534.
+// Packed surface key of a Hit record: (int) id + 1 and (int) tree + 1 in 16
+// bits each, or -1 (never a packed key) unless both lie in [0, 65535) or are
+// exactly -1 (what tracePixels writes); the truncations are kMagic adds
+// rounded toward zero.
+__device__ __forceinline__ bool key_range(float v) { return (v >= 0.0f || v == -1.0f) && v < 65535.0f; }
 __device__ __forceinline__ int surface_key(float id_f, float tree_f) {
-  const int id = (int)id_f, tree = (int)tree_f;
-  if (id < -1 || id > 65534 || tree < -1 || tree > 65534) return -1;
+  if (!key_range(id_f) || !key_range(tree_f)) return -1;
+  const int id = __float_as_int(__fadd_rz(id_f, kMagic)) - kMagicBits, tree = __float_as_int(__fadd_rz(tree_f, kMagic)) - kMagicBits;
   return (id + 1) | ((tree + 1) << 16);
 }
 
-template <bool kResolve>
-__device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restrict__ Linear, const float* __restrict__ Guide,
-                                            const float* __restrict__ Hit, float* __restrict__ Filtered, float* __restrict__ History,
-                                            uint32_t* __restrict__ Pixels, float c9, float c10, float c15, float c20, int width, int height,
-                                            int x0, int y0) {
-  const int tid = threadIdx.y * kFX + threadIdx.x;
-  // Filter weights expf(-(j*j+k*k)*0.30f) for r^2 = 0, 1, 2, 4, 5, 8.
+// Filter weights expf(-(j*j+k*k)*0.30f) for r^2 = 0, 1, 2, 4, 5, 8, staged by
+// the first six threads.
+__device__ __forceinline__ void filter_weights(FilterTile& s, int tid) {
   if (tid < 6) {
     const int r2[6] = {0, 1, 2, 4, 5, 8};
     s.w[tid] = xexp(-(float)r2[tid] * 0.30f);
   }
+}
+
+// One staged halo pixel: its depth bits, packed key and demodulated colour.
+// Returns false when its ids do not fit the packed key.
+__device__ __forceinline__ bool filter_stage_px(FilterTile& s, int sy, int sx, float4 h, float4 l, float4 g) {
+  const int key = surface_key(h.y, h.z);
+  s.key[sy][sx] = make_int2(__float_as_int(h.x), key);
+  s.demod[sy][sx] = make_float4(l.x / (g.x + 0.02f), l.y / (g.y + 0.02f), l.z / (g.z + 0.02f), 0.0f);
+  return key >= 0;
+}
+
+// Stage a tile's halo from global memory.  Returns (uniformly over the CTA)
+// whether some staged id does not fit the packed key.
+// All of a thread's staging loads are issued before any is used, so their
+// latencies overlap.  The vignette coordinates of the tile's columns and
+// rows are computed once here (kResolve).
+template <bool kResolve>
+__device__ __forceinline__ bool filter_stage_global(FilterTile& s, const float* __restrict__ Linear, const float* __restrict__ Guide,
+                                                    const float* __restrict__ Hit, int width, int height, int x0, int y0, int tid) {
+  filter_weights(s, tid);
+  if (kResolve) {
+    if (tid >= 32 && tid < 32 + kFX) s.u[tid - 32] = vig_coord(x0 + tid - 32, width);
+    if (tid >= 64 && tid < 64 + kFY) s.v[tid - 64] = vig_coord(y0 + tid - 64, height);
+  }
   const int hx0 = x0 - kHalo, hy0 = y0 - kHalo;
-  bool unpacked = false;
-  for (int k = tid; k < kSX * kSY; k += kFX * kFT) {
+  constexpr int kPer = (kSX * kSY + kFX * kFT - 1) / (kFX * kFT);
+  float4 hv[kPer], lv[kPer], gv[kPer];
+  bool in[kPer];
+#pragma unroll
+  for (int n = 0; n < kPer; n++) {
+    const int k = tid + n * kFX * kFT;
     const int sy = k / kSX, sx = k - sy * kSX;
     const int gx = hx0 + sx, gy = hy0 + sy;
-    if (gx >= 0 && gy >= 0 && gx < width && gy < height) {
+    in[n] = k < kSX * kSY && gx >= 0 && gy >= 0 && gx < width && gy < height;
+    if (in[n]) {
       const int q = gy * width + gx;
-      const float4 h = __ldg(reinterpret_cast<const float4*>(Hit) + q);
-      const float4 l = __ldg(reinterpret_cast<const float4*>(Linear) + q);
-      const float4 g = __ldg(reinterpret_cast<const float4*>(Guide) + q);
-      const int key = surface_key(h.y, h.z);
-      unpacked |= key < 0;
-      s.key[sy][sx] = make_int2(__float_as_int(h.x), key);
-      s.demod[sy][sx] = make_float4(l.x / (g.x + 0.02f), l.y / (g.y + 0.02f), l.z / (g.z + 0.02f), 0.0f);
+      hv[n] = __ldg(reinterpret_cast<const float4*>(Hit) + q);
+      lv[n] = __ldg(reinterpret_cast<const float4*>(Linear) + q);
+      gv[n] = __ldg(reinterpret_cast<const float4*>(Guide) + q);
     }
   }
-  unpacked = __syncthreads_or(unpacked);
+  bool unpacked = false;
+#pragma unroll
+  for (int n = 0; n < kPer; n++) {
+    const int k = tid + n * kFX * kFT;
+    const int sy = k / kSX, sx = k - sy * kSX;
+    if (in[n]) unpacked |= !filter_stage_px(s, sy, sx, hv[n], lv[n], gv[n]);
+  }
+  return __syncthreads_or(unpacked);
+}
+
+// The centre values of a pair's pixel e, read from global memory.
+struct CentreGlobal {
+  const float* Linear;
+  const float* Guide;
+  const float* Hit;
+  int i0, width;
+  __device__ __forceinline__ int index(int e) const { return e ? i0 + width : i0; }
+  __device__ __forceinline__ float4 linear(int e) const { return __ldg(reinterpret_cast<const float4*>(Linear) + index(e)); }
+  __device__ __forceinline__ float4 guide(int e) const { return __ldg(reinterpret_cast<const float4*>(Guide) + index(e)); }
+  __device__ __forceinline__ float footprint(int e) const { return __ldg(Hit + 4 * index(e) + 3); }
+};
+
+// Filter the staged tile: each thread its vertical pair of pixels, then
+// (kResolve) resolvePixels on the filtered values.
+template <bool kResolve, class Centre>
+__device__ __forceinline__ void filter_finish(const FilterTile& s, bool unpacked, const Centre& ctr, const float* __restrict__ Linear,
+                                              const float* __restrict__ Guide, const float* __restrict__ Hit, float* __restrict__ Filtered,
+                                              float* __restrict__ History, uint32_t* __restrict__ Pixels, float c9, float c10, float c15, float c20,
+                                              int width, int height, int x0, int y0) {
   const float w[6] = {s.w[0], s.w[1], s.w[2], s.w[3], s.w[4], s.w[5]};
   const int x = x0 + threadIdx.x, y = y0 + 2 * threadIdx.y;
   if (x >= width || y >= height) return;
+  const float count = sample_count(c9, c10);
+  const float inv = kResolve ? 1.0f / (count + 1.0f) : 0.0f;
   const int cx = threadIdx.x + kHalo, cy = 2 * threadIdx.y + kHalo;
   const bool has1 = y + 1 < height;
   const int i0 = y * width + x, i1 = i0 + width;
@@ -684,7 +758,7 @@ __device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restri
     p[e].sum = mk(0.0f, 0.0f, 0.0f);
     p[e].weight = 0.0f;
     live[e] = filter && (e == 0 || has1) && p[e].depth < kFar;
-    p[e].tol = live[e] ? fmaxf(0.005f, __ldg(Hit + 4 * (e ? i1 : i0) + 3) * 6.0f) : 0.0f;
+    p[e].tol = live[e] ? fmaxf(0.005f, ctr.footprint(e) * 6.0f) : 0.0f;
   }
   f3 col[2];
   if (!unpacked) {
@@ -698,11 +772,10 @@ __device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restri
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       if (e == 1 && !has1) break;
-      const int i = e ? i1 : i0;
-      const float4 lc = __ldg(reinterpret_cast<const float4*>(Linear) + i);
+      const float4 lc = ctr.linear(e);
       col[e] = mk(lc.x, lc.y, lc.z);
       if (live[e] && p[e].weight > 0.0f) {
-        const float4 gc = __ldg(reinterpret_cast<const float4*>(Guide) + i);
+        const float4 gc = ctr.guide(e);
         const f3 base = mk(gc.x, gc.y, gc.z) + mk(0.02f, 0.02f, 0.02f);
         col[e] = mix3(col[e], (p[e].sum / p[e].weight) * base, 0.86f);
       }
@@ -711,11 +784,10 @@ __device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restri
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       if (e == 1 && !has1) break;
-      const int i = e ? i1 : i0;
       if (live[e]) {
         col[e] = filter_px_direct(Linear, Guide, Hit, x, y + e, width, height);
       } else {
-        const float4 lc = __ldg(reinterpret_cast<const float4*>(Linear) + i);
+        const float4 lc = ctr.linear(e);
         col[e] = mk(lc.x, lc.y, lc.z);
       }
     }
@@ -724,8 +796,20 @@ __device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restri
   for (int e = 0; e < 2; e++) {
     if (e == 1 && !has1) break;
     reinterpret_cast<float4*>(Filtered)[e ? i1 : i0] = make_float4(col[e].x, col[e].y, col[e].z, 1.0f);
-    if (kResolve) resolve_px(col[e], History, Pixels, c9, c10, c20, x, y + e, width, height);
+    if (kResolve) resolve_px(col[e], History, Pixels, count, inv, c20, s.u[threadIdx.x], s.v[2 * threadIdx.y + e], e ? i1 : i0);
   }
+}
+
+template <bool kResolve>
+__device__ __forceinline__ void filter_tile(FilterTile& s, const float* __restrict__ Linear, const float* __restrict__ Guide,
+                                            const float* __restrict__ Hit, float* __restrict__ Filtered, float* __restrict__ History,
+                                            uint32_t* __restrict__ Pixels, float c9, float c10, float c15, float c20, int width, int height,
+                                            int x0, int y0) {
+  const int tid = threadIdx.y * kFX + threadIdx.x;
+  const bool unpacked = filter_stage_global<kResolve>(s, Linear, Guide, Hit, width, height, x0, y0, tid);
+  const int i0 = (y0 + 2 * (int)threadIdx.y) * width + x0 + (int)threadIdx.x;
+  const CentreGlobal ctr{Linear, Guide, Hit, i0, width};
+  filter_finish<kResolve>(s, unpacked, ctr, Linear, Guide, Hit, Filtered, History, Pixels, c9, c10, c15, c20, width, height, x0, y0);
 }
 
 }  // namespace

@@ -219,11 +219,13 @@ __global__ void __launch_bounds__(kBlock) shade_inorder_kernel(const float* __re
   reinterpret_cast<float4*>(Guide)[pixel] = make_float4(sh.guide.x, sh.guide.y, sh.guide.z, 1.0f);
 }
 
+// filterLighting (+ resolvePixels) of one 32x16 tile per CTA, its halo
+// staged from global memory; 4 CTAs per SM.
 template <bool kResolve>
-__global__ void __launch_bounds__(kFX * kFT, 3) filter_kernel(const float* __restrict__ Linear, const float* __restrict__ Guide,
-                                                           const float* __restrict__ Hit, float* __restrict__ Filtered,
-                                                           float* __restrict__ History, uint32_t* __restrict__ Pixels,
-                                                           const float* __restrict__ C, int width, int height) {
+__global__ void __launch_bounds__(kFX * kFT, 4) filter_kernel(const float* __restrict__ Linear, const float* __restrict__ Guide,
+                                                              const float* __restrict__ Hit, float* __restrict__ Filtered,
+                                                              float* __restrict__ History, uint32_t* __restrict__ Pixels,
+                                                              const float* __restrict__ C, int width, int height) {
   __shared__ FilterTile s;
   filter_tile<kResolve>(s, Linear, Guide, Hit, Filtered, History, Pixels, kResolve ? C[9] : 0.0f, kResolve ? C[10] : 0.0f, C[15],
                         kResolve ? C[20] : 0.0f, width, height, blockIdx.x * kFX, blockIdx.y * kFY);
@@ -237,7 +239,8 @@ __global__ void __launch_bounds__(kRX * kRY) resolve_kernel(const float* __restr
   const int x = blockIdx.x * kRX + threadIdx.x, y = blockIdx.y * kRY + threadIdx.y;
   if (x >= width || y >= height) return;
   float4 f = __ldg(reinterpret_cast<const float4*>(Filtered) + y * width + x);
-  resolve_px(mk(f.x, f.y, f.z), History, Pixels, C[9], C[10], C[20], x, y, width, height);
+  const float count = sample_count(C[9], C[10]);
+  resolve_px(mk(f.x, f.y, f.z), History, Pixels, count, 1.0f / (count + 1.0f), C[20], vig_coord(x, width), vig_coord(y, height), y * width + x);
 }
 
 // Dynamic shared memory of a 256-thread CTA: one WarpBatch per warp.
@@ -272,6 +275,18 @@ dim3 pool_grid(int w, int h) {
   return dim3((unsigned)std::min<long>(blocks, 2L * sms[dev]));
 }
 dim3 filter_grid(int w, int h) { return dim3((w + kFX - 1) / kFX, (h + kFY - 1) / kFY); }
+
+// filterLighting (+ resolvePixels) over width x height: one 32x16 tile per CTA.
+int launch_filter(const char* name, bool resolve, const float* Linear, const float* Guide, const float* Hit, float* Filtered, float* History,
+                  uint32_t* Pixels, const float* C, int width, int height, cudaStream_t stream) {
+  if (resolve)
+    filter_kernel<true><<<filter_grid(width, height), dim3(kFX, kFT), 0, stream>>>(Linear, Guide, Hit, Filtered, History, Pixels, C, width, height);
+  else
+    filter_kernel<false><<<filter_grid(width, height), dim3(kFX, kFT), 0, stream>>>(Linear, Guide, Hit, Filtered, nullptr, nullptr, C, width,
+                                                                                    height);
+  count_launch();
+  return check_launch(name);
+}
 dim3 resolve_grid(int w, int h) { return dim3((w + kRX - 1) / kRX, (h + kRY - 1) / kRY); }
 
 int trace_entry(const char* name, bool forest, const float* P, const float* Nodes, const uint32_t* Order, const float* C, float* Hit, int width,
@@ -478,10 +493,7 @@ extern "C" int arbor_filterLighting(const float* Linear, const float* Guide, con
                        {C, kC, false, 4, "C"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
-  filter_kernel<false><<<filter_grid(width, height), dim3(kFX, kFT), 0, stream>>>(Linear, Guide, Hit, Filtered, nullptr, nullptr, C, width,
-                                                                                  height);
-  count_launch();
-  return check_launch(name);
+  return launch_filter(name, false, Linear, Guide, Hit, Filtered, nullptr, nullptr, C, width, height, stream);
 }
 extern "C" int arbor_resolvePixels(const float* Filtered, float* History, uint32_t* Pixels, const float* C, int width, int height,
                                    arbor_stream stream) {
@@ -511,8 +523,6 @@ extern "C" int arbor_filterResolve(const float* Linear, const float* Guide, cons
                        {C, kC, false, 4, "C"}};
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
-  filter_kernel<true><<<filter_grid(width, height), dim3(kFX, kFT), 0, stream>>>(Linear, Guide, Hit, Filtered, History, Pixels, C, width,
-                                                                                 height);
-  count_launch();
-  return check_launch(name);
+  return launch_filter(name, true, Linear, Guide, Hit, Filtered, History, Pixels, C, width, height, stream);
 }
+

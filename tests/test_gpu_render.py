@@ -340,3 +340,38 @@ def test_resolve_bytes_match_double_precision_gamma(cuda, gu):
     want = b[:, 0] | (b[:, 1] << 8) | (b[:, 2] << 16) | np.uint32(0xFF000000)
     print(f"[gamma bytes] {np.count_nonzero(got != want)} of {w * h} pixels differ")
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("w,h", [(36, 20), (37, 23), (35, 19), (200, 120), (33, 1000), (1920, 1080)])
+def test_filter_sizes_exact(cuda, oracle, gu, w, h):
+    """filterLighting and filterResolve on random surfaces at sizes around
+    and above one 32x16 tile with its halo: Filtered and History bit-exact
+    against the oracle, Pixels within 1 LSB."""
+    rng = np.random.default_rng(w * 7 + h)
+    hit = np.zeros((h * w, 4), np.float32)
+    hit[:, 0] = rng.uniform(1.0, 60.0, h * w).astype(np.float32)
+    hit[:, 1] = rng.integers(-1, 6, h * w)  # few ids: many same-surface neighbours
+    hit[:, 2] = rng.integers(-1, 3, h * w)
+    hit[:, 3] = rng.uniform(0.0, 0.01, h * w).astype(np.float32)
+    hit[rng.random(h * w) < 0.05, 0] = 1e5  # sky
+    hit = hit.reshape(-1)
+    lin = (rng.random(w * h * 4) * 2.0).astype(np.float32)
+    gui = rng.random(w * h * 4).astype(np.float32)
+    C = np.zeros(64, np.float32)
+    C[9], C[10], C[20] = 2.0, 0.0, 1.18
+    filt_ref = oracle.filter(lin, gui, hit, C, w, h)
+    hist0 = rng.random(w * h * 4).astype(np.float32)
+    hist_ref = hist0.copy()
+    px_ref = oracle.resolve(filt_ref, hist_ref, C, w, h)
+    dl, dg, dh, dC = gu.dev(lin), gu.dev(gui), gu.dev(hit), gu.dev(C)
+    filt = gu.zeros_f(w * h * 4)
+    gu.ok(cuda.call("arbor_filterLighting", dl, dg, dh, filt, dC, w, h))
+    filt2, hist, px = gu.zeros_f(w * h * 4), gu.dev(hist0), gu.zeros_u(w * h)
+    gu.ok(cuda.call("arbor_filterResolve", dl, dg, dh, filt2, hist, px, dC, w, h))
+    assert np.array_equal(u32(gu.host(filt)), u32(filt_ref))
+    assert np.array_equal(u32(gu.host(filt2)), u32(filt_ref))
+    assert np.array_equal(u32(gu.host(hist)), u32(hist_ref))
+    got = gu.host(px, np.uint32)
+    diff = np.max(np.abs(np.stack([(got >> s_) & 255 for s_ in (0, 8, 16, 24)]).astype(int)
+                         - np.stack([(px_ref >> s_) & 255 for s_ in (0, 8, 16, 24)]).astype(int)), 0)
+    assert diff.max() <= 1
