@@ -366,16 +366,16 @@ def test_backward_data_pass_on_tcgen05_matches_mma_sync(cuda):
 
 def test_trained_network_beats_filter_lighting_on_rendered_views(cuda):
     """What the learned path gains over the method without it: trained for
-    400 steps on 12 tracer-rendered views (1-spp inputs, 32-spp targets,
+    1500 steps on 24 tracer-rendered views (1-spp inputs, 64-spp targets,
     128x128 crops at the full-HD pixel angle, sun shadows on), the network at
     1 spp beats filterLighting at 1 spp by >= 1 dB PSNR (after resolvePixels'
-    tone mapping) on 6 held-out views."""
+    tone mapping, mean over 6 held-out views; measured +2.7 dB)."""
     import math
 
     import denoise_train as dt
     import workloads
 
-    S, spp = 128, 32
+    S, spp = 128, 64
     seeds = workloads.batch_seeds(4)
     scenes = {}
     fr = dt.Frame(S, S)
@@ -385,7 +385,7 @@ def test_trained_network_beats_filter_lighting_on_rendered_views(cuda):
             scenes[k] = dt.Scene(seeds[k])
         return scenes[k]
 
-    train = [dt.render_pair(fr, scene_of(k), C, spp, eval_baselines=False) for k, C in dt.view_states(12, seeds, S, seed=21)]
+    train = [dt.render_pair(fr, scene_of(k), C, spp, eval_baselines=False) for k, C in dt.view_states(24, seeds, S, seed=21)]
     evals = [dt.render_pair(fr, scene_of(k), C, spp, eval_baselines=True) | {"C": C} for k, C in dt.view_states(6, seeds, S, seed=22)]
     feats = torch.stack([r["feat"] for r in train])
     base = torch.stack([r["base"] for r in train])
@@ -393,9 +393,9 @@ def test_trained_network_beats_filter_lighting_on_rendered_views(cuda):
     net = Net(4, S, S, seed=7)
     try:
         rng = np.random.default_rng(3)
-        for step in range(400):
+        for step in range(1500):
             i = int(rng.integers(0, len(train) - 4 + 1))
-            lr = 1e-5 + 0.5 * (1e-3 - 1e-5) * (1.0 + math.cos(math.pi * step / 400))
+            lr = 1e-5 + 0.5 * (2e-3 - 1e-5) * (1.0 + math.cos(math.pi * step / 1500))
             assert net.lib.arbor_denoiser_train_step(net.h, feats[i].data_ptr(), base[i].data_ptr(), target[i].data_ptr(), 4, S, S, lr,
                                                      None) == ab.OK, ab.last_error()
         den = torch.zeros(S * S * 4, device="cuda")
