@@ -3,6 +3,7 @@ GPU by the library's own kernels, and evaluation against filterLighting.
 
     python arbor-cuda_b200/denoise_train.py [--train-views 96] [--eval-views 64]
         [--size 384] [--spp 256] [--steps 1500] [--batch 4] [--out results.json]
+        [--eval-width 1920 --eval-height 1080] [--eval-spp 64]
 
 Data: views of the 324-tree forest from 16 master seeds at random poses
 (1.72 m eye height, sun shadows on), `size` x `size` pixels with the
@@ -16,7 +17,9 @@ target: the mean of Linear over `spp` samples.
 The network corrects filterLighting's 1-spp output (its base image) using
 the features; training minimises L1 in log(1 + radiance).
 
-Evaluation, on held-out views (other poses): PSNR against the `spp` target
+Evaluation, on held-out views (other poses; full frames of --eval-width x
+--eval-height at C[14] = 0.9 when given, else crops like the training views,
+with an --eval-spp target): PSNR against the target
 after resolvePixels' tone mapping (exposure, ACES, gamma 1/2.2, vignette;
 Arbor.cu:303-304, before quantisation), of
   - filterLighting at 1 spp (Filtered),
@@ -85,11 +88,14 @@ class Frame:
             check(ab.call("arbor_shadePixels", scene.P, scene.Nodes, scene.Order, self.C, self.Hit, self.Lin, self.Gui, w, h))
 
 
-def view_states(n: int, seeds: list[int], size: int, seed: int) -> list[tuple[int, np.ndarray]]:
+def view_states(n: int, seeds: list[int], size: int, seed: int, full: tuple[int, int] | None = None) -> list[tuple[int, np.ndarray]]:
+    """n seeded views: size x size crops at the pixel angle of a 1080-row
+    frame, or (full = (w, h)) whole frames at the reference's C[14] = 0.9."""
     out = []
-    for scene, w, h, C in workloads.batch_views(n, seeds, resolutions=((size, size),), seed=seed, shadows=True):
+    res = ((full[0], full[1]),) if full else ((size, size),)
+    for scene, w, h, C in workloads.batch_views(n, seeds, resolutions=res, seed=seed, shadows=True):
         C = C.copy()
-        C[14] = np.float32(0.9 * size / 1080.0)  # the pixel angle of a 1080-row frame
+        C[14] = np.float32(0.9 if full else 0.9 * size / 1080.0)  # the pixel angle of a 1080-row frame
         out.append((scene, C))
     return out
 
@@ -157,6 +163,9 @@ def main() -> None:
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--scenes", type=int, default=16)
     ap.add_argument("--hflip", action="store_true", help="add the mirrored training views (horizontal flip) to the training set")
+    ap.add_argument("--eval-width", type=int, default=0, help="evaluate on whole frames of this size (with --eval-height)")
+    ap.add_argument("--eval-height", type=int, default=0)
+    ap.add_argument("--eval-spp", type=int, default=0, help="samples of the evaluation target (default --spp)")
     ap.add_argument("--out", default="")
     args = ap.parse_args()
     torch.cuda.init()
@@ -173,7 +182,10 @@ def main() -> None:
         return scenes[k]
 
     train_views = view_states(args.train_views, seeds, S, seed=11)
-    eval_views = view_states(args.eval_views, seeds, S, seed=12)
+    full = (args.eval_width, args.eval_height) if args.eval_width and args.eval_height else None
+    EW, EH = full if full else (S, S)
+    eval_spp = args.eval_spp or args.spp
+    eval_views = view_states(args.eval_views, seeds, S, seed=12, full=full)
     px = S * S
     feats = torch.zeros(args.train_views, px * 16, dtype=torch.int16, device="cuda")
     base = torch.zeros(args.train_views, px * 4, device="cuda")
@@ -181,7 +193,10 @@ def main() -> None:
     for i, (k, C) in enumerate(train_views):
         r = render_pair(fr, scene_of(k), C, args.spp, eval_baselines=False)
         feats[i], base[i], target[i] = r["feat"], r["base"], r["target"]
-    evals = [render_pair(fr, scene_of(k), C, args.spp, eval_baselines=True) | {"C": C} for k, C in eval_views]
+    efr = Frame(EW, EH) if full else fr
+    evals = []
+    for k, C in eval_views:
+        evals.append(render_pair(efr, scene_of(k), C, eval_spp, eval_baselines=True) | {"C": C})
     n_train = args.train_views
     if args.hflip:
         # mirrored copies (every channel keeps its meaning; only the image's
@@ -212,17 +227,28 @@ def main() -> None:
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
 
-    # evaluation
-    den = torch.zeros(px * 4, device="cuda")
+    # evaluation (whole frames: a second denoiser of that size with the trained parameters)
+    he = h
+    if full:
+        n_par = ctypes.c_size_t()
+        check(lib.arbor_denoiser_param_count(h, ctypes.byref(n_par)))
+        params = np.zeros(n_par.value, np.float32)
+        check(lib.arbor_denoiser_get_params(h, params.ctypes.data, params.size))
+        he = ctypes.c_void_p()
+        check(lib.arbor_denoiser_create(ctypes.byref(he), 1, EW, EH, 7, None))
+        check(lib.arbor_denoiser_set_params(he, params.ctypes.data, params.size))
+    den = torch.zeros(EW * EH * 4, device="cuda")
     scores = {"noisy_1spp": [], "filter_1spp": [], "filter_4spp": [], "denoiser_1spp": []}
     for e in evals:
-        check(lib.arbor_denoiser_infer(h, e["feat"].data_ptr(), e["base"].data_ptr(), den.data_ptr(), S, S))
+        check(lib.arbor_denoiser_infer(he, e["feat"].data_ptr(), e["base"].data_ptr(), den.data_ptr(), EW, EH))
         exposure = float(e["C"][20])
-        ref = tonemap(e["target"], S, S, exposure)
-        scores["noisy_1spp"].append(psnr(tonemap(e["noisy"], S, S, exposure), ref))
-        scores["filter_1spp"].append(psnr(tonemap(e["filter1"], S, S, exposure), ref))
-        scores["filter_4spp"].append(psnr(tonemap(e["filter4"], S, S, exposure), ref))
-        scores["denoiser_1spp"].append(psnr(tonemap(den, S, S, exposure), ref))
+        ref = tonemap(e["target"], EW, EH, exposure)
+        scores["noisy_1spp"].append(psnr(tonemap(e["noisy"], EW, EH, exposure), ref))
+        scores["filter_1spp"].append(psnr(tonemap(e["filter1"], EW, EH, exposure), ref))
+        scores["filter_4spp"].append(psnr(tonemap(e["filter4"], EW, EH, exposure), ref))
+        scores["denoiser_1spp"].append(psnr(tonemap(den, EW, EH, exposure), ref))
+    if full:
+        check(lib.arbor_denoiser_destroy(he))
     check(lib.arbor_denoiser_destroy(h))
 
     # frame times at 1920x1080
@@ -250,9 +276,10 @@ def main() -> None:
     mean = {k: round(float(np.mean(v)), 3) for k, v in scores.items()}
     result = {
         "denoiser": "4-level U-Net 32/64/96/128, 3x3, BF16 weights and activations, FP32 accumulation; forward "
-                    "convolutions on tcgen05 (TMEM accumulators), backward on mma.sync m16n8k16",
+                    "convolutions and most of the backward data pass on tcgen05 (TMEM accumulators), weight gradients on "
+                    "mma.sync m16n8k16 folded in a fixed order",
         "data": {"train_views": args.train_views, "eval_views": args.eval_views, "size": S, "spp_target": args.spp, "scenes": args.scenes, "hflip": bool(args.hflip),
-                 "render_seconds": round(t_data, 1)},
+                 "eval_size": [EW, EH], "eval_spp_target": eval_spp, "render_seconds": round(t_data, 1)},
         "train": {"steps": args.steps, "batch": args.batch, "lr": args.lr, "seconds": round(t_train, 2),
                   "ms_per_step": round(1e3 * t_train / max(1, args.steps), 3), "loss": losses},
         "psnr_db_mean": mean,
