@@ -134,6 +134,7 @@ SIGNATURES = {
     "arbor_denoiser_gradient": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, ctypes.c_size_t, ctypes.POINTER(_f)]),
     "arbor_denoiser_infer": (_i, [_vp, _vp, _vp, _vp, _i, _i]),
     "arbor_denoiser_set_backend": (_i, [_vp, _i]),
+    "arbor_denoiser_set_loss": (_i, [_vp, _i]),
     "arbor_denoiser_check": (_i, [_vp]),
     "arbor_denoiser_destroy": (_i, [_vp]),
     "arbor_accumulate": (_i, [_vp, _vp, ctypes.c_size_t, _f, _vp]),

@@ -12,6 +12,8 @@
 //                        per pixel or per scene (generation, camera, instance
 //                        table, sun direction, sky, tone curve), so those
 //                        values agree with a correctly rounded CPU libm.
+//                        The per-tree yaw sines and cosines come from the
+//                        host's libm instead (WorldTrig below).
 //   sinf/cosf/expf/powf/atan2f  CUDA's single-precision functions, used in
 //                        the inner loops (SDF march, Newton solve, bark).
 #pragma once
@@ -84,8 +86,8 @@ __host__ __device__ __forceinline__ uint32_t hashU(uint32_t x) {
   x ^= x >> 16;
   return x;
 }
-__device__ __forceinline__ float unit24(uint32_t h) { return (float)(h & 16777215u) / 16777216.0f; }
-__device__ __forceinline__ float rnd(int n, int seed) { return unit24(hashU((uint32_t)n ^ hashU((uint32_t)seed))); }
+__host__ __device__ __forceinline__ float unit24(uint32_t h) { return (float)(h & 16777215u) / 16777216.0f; }
+__host__ __device__ __forceinline__ float rnd(int n, int seed) { return unit24(hashU((uint32_t)n ^ hashU((uint32_t)seed))); }
 // rnd with the seed hash precomputed: rndh(n, hashU(seed)) == rnd(n, seed).
 __device__ __forceinline__ float rndh(int n, uint32_t hseed) { return unit24(hashU((uint32_t)n ^ hseed)); }
 __device__ __forceinline__ int hcell(int x, int y) { return (int)((uint32_t)x * 1973u + (uint32_t)y * 9277u); }
@@ -157,7 +159,7 @@ __device__ __forceinline__ float halton(int n, int base) {
 }
 
 // Forest instancing (Arbor.cu:57-66).
-__device__ __forceinline__ int forest_seed(int tree, int ws) {
+__host__ __device__ __forceinline__ int forest_seed(int tree, int ws) {
   return (int)(hashU((uint32_t)tree * 92821u + (uint32_t)ws * 68917u + 17u) & 1048575u);
 }
 __device__ __forceinline__ f3 forest_pos(int tree, int ws) {
@@ -171,7 +173,7 @@ __device__ __forceinline__ f3 forest_pos(int tree, int ws) {
   return mk((float)x * kSpacing + jx + warpX, 0.0f, (float)z * kSpacing + jz + warpZ);
 }
 __device__ __forceinline__ float forest_scale(int tree, int ws) { return 0.72f + rnd(3, forest_seed(tree, ws)) * 0.62f; }
-__device__ __forceinline__ float forest_yaw(int tree, int ws) { return rnd(4, forest_seed(tree, ws)) * kPi * 2.0f; }
+__host__ __device__ __forceinline__ float forest_yaw(int tree, int ws) { return rnd(4, forest_seed(tree, ws)) * kPi * 2.0f; }
 
 // One forest instance, precomputed per tree: every value is what the
 // reference's forest helpers (Arbor.cu:57-69, 246-247, 279-282) compute on
@@ -206,6 +208,53 @@ __device__ __forceinline__ Instance make_instance(int tree, int ws) {
   return t;
 }
 // Arbor.cu:67-69
+// The per-tree yaw sines and cosines of a world seed as the reference
+// harness computes them: sinf/cosf of the host's C library (Arbor.cu:67-69
+// compiled for the CPU).  That library's single-precision sine and cosine are
+// not correctly rounded: for about 3 % of the trees one of the four values is
+// one unit in the last place away from make_instance's correctly rounded
+// one, which turns the tree by that much and changes hit IDs along its
+// silhouettes.  The host fills a registry slot per world seed
+// (register_world_seed, camera.cu) and block prologues take the four values
+// from it; a seed without a slot keeps make_instance's values.
+constexpr int kTrigSlots = 64;
+struct WorldTrig {
+  int ws, ready;        // world seed; 1 once the values below are in place
+  int pad[2];
+  float4 v[kForest];    // per tree: cos(-yaw), sin(-yaw), cos(yaw), sin(yaw)
+};
+// Host: the registry of the current device (nullptr if it cannot be
+// allocated) and the registration of a world seed (a no-op for a seed already
+// present, with the registry full, or while `stream` is being captured).
+const WorldTrig* world_trig();
+void register_world_seed(int ws, cudaStream_t stream);
+
+// Block-wide: the registry's values for world seed ws, or nullptr.  Every
+// thread of the block calls it (it synchronises the block).
+__device__ __forceinline__ const float4* world_trig_of(const WorldTrig* trig, int ws) {
+  __shared__ int slot;
+  if (threadIdx.x == 0) slot = -1;
+  __syncthreads();
+  if (trig != nullptr && threadIdx.x < kTrigSlots) {
+    const volatile WorldTrig* s = trig + threadIdx.x;
+    if (s->ready == 1 && s->ws == ws) atomicMax(&slot, (int)threadIdx.x);
+  }
+  __syncthreads();
+  return slot >= 0 ? trig[slot].v : nullptr;
+}
+// make_instance with the registry's sines and cosines where it has them.
+__device__ __forceinline__ Instance make_instance(int tree, int ws, const float4* yaw_trig) {
+  Instance t = make_instance(tree, ws);
+  if (yaw_trig != nullptr) {
+    const float4 q = yaw_trig[tree];
+    t.lc = q.x;
+    t.ls = q.y;
+    t.wc = q.z;
+    t.wsn = q.w;
+  }
+  return t;
+}
+
 __device__ __forceinline__ f3 to_local_point(f3 p, const Instance& t) {
   f3 q = mk(p.x - t.px, p.y - 0.0f, p.z - t.pz);
   return mk(q.x * t.lc - q.z * t.ls, q.y, q.x * t.ls + q.z * t.lc) / t.sc;

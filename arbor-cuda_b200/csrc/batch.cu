@@ -59,8 +59,8 @@ struct BatchView {
   int width, height;
 };
 
-__global__ void __launch_bounds__(kBlock) batch_setup_kernel(const float* __restrict__ Cs, Camera* __restrict__ cams, float4* __restrict__ scal,
-                                                             Instance* __restrict__ insts, int* __restrict__ counters) {
+__global__ void __launch_bounds__(kBlock) batch_setup_kernel(const float* __restrict__ Cs, const WorldTrig* __restrict__ trig, Camera* __restrict__ cams,
+                                                             float4* __restrict__ scal, Instance* __restrict__ insts, int* __restrict__ counters) {
   const int v = blockIdx.x;
   if (threadIdx.x == 0) {
     counters[kViewQueues + v] = 0;
@@ -74,7 +74,8 @@ __global__ void __launch_bounds__(kBlock) batch_setup_kernel(const float* __rest
     scal[v] = make_float4(C[9], C[10], C[15], C[20]);
   }
   const int ws = (int)C[31];
-  for (int t = threadIdx.x; t < kForest; t += blockDim.x) insts[v * kForest + t] = make_instance(t, ws);
+  const float4* yaw_trig = world_trig_of(trig, ws);
+  for (int t = threadIdx.x; t < kForest; t += blockDim.x) insts[v * kForest + t] = make_instance(t, ws, yaw_trig);
   if (v == 0 && threadIdx.x < kViewQueues) counters[threadIdx.x] = 0;
 }
 
@@ -244,7 +245,7 @@ std::vector<int> view_order(const arbor_batch* b, const std::vector<int>& subset
 }
 
 int launch_setup(arbor_batch* b, cudaStream_t s) {
-  batch_setup_kernel<<<b->n_views, kBlock, 0, s>>>(b->C, b->cams, b->scal, b->insts, b->counters);
+  batch_setup_kernel<<<b->n_views, kBlock, 0, s>>>(b->C, world_trig(), b->cams, b->scal, b->insts, b->counters);
   return check_launch("batch_setup_kernel");
 }
 

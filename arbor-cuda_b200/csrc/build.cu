@@ -536,6 +536,7 @@ extern "C" int arbor_buildScene(int seed, float* B, float* P, uint32_t* Keys, ui
                          {Keys, kKeys, true, 4, "Keys"}, {Order, kKeys, true, 4, "Order"}, {scratch, arbor_sort_scratch_bytes(), true, 4, "scratch"}};
     if (int s = check_bindings("arbor_buildScene", c)) return s;
   }
+  register_world_seed(seed, stream);  // a forest built from `seed` has world seed `seed` (initCamera sets C[31])
   if (int s = launch_grow_all(B, seed, stream)) return s;
   if (int s = launch_prims_keys(B, P, Keys, Order, seed, stream)) return s;
   if (int s = launch_sort(Keys, Order, scratch, stream)) return s;

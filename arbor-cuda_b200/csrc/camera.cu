@@ -5,6 +5,9 @@
 // 9 sample index, 10 history reset, 11 wind amplitude, 12/13 sun azimuth /
 // elevation, 14 FOV scale, 15 view mode, 16/17 yaw/pitch, 20 exposure,
 // 22 shadows, 24 frame counter, 31 world seed, 32/33 width/height.
+#include <cmath>
+#include <mutex>
+
 #include "abi_util.h"
 #include "arbor_math.cuh"
 
@@ -117,12 +120,88 @@ __global__ void set_sample_kernel(float* C, int sample, int reset) {
 
 // The forest instance table of world seed ws, one Instance per tree: the
 // table every trace/shade CTA builds in shared memory (render_common.cuh).
-__global__ void forest_instances_kernel(Instance* out, int ws) {
+__global__ void forest_instances_kernel(Instance* out, int ws, const WorldTrig* trig) {
+  const float4* yaw_trig = world_trig_of(trig, ws);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < kForest) out[t] = make_instance(t, ws);
+  if (t < kForest) out[t] = make_instance(t, ws, yaw_trig);
+}
+
+// Per-device registry of world-seed yaw tables (WorldTrig).  Slots are
+// written once, data before header, and never reused, so a kernel running
+// on another stream meanwhile reads either a complete slot or none.
+struct TrigRegistry {
+  WorldTrig* dev = nullptr;
+  int used = 0;
+  int seeds[kTrigSlots];
+};
+constexpr int kMaxDevices = 64;
+std::mutex g_trig_mu;
+TrigRegistry g_trig[kMaxDevices];
+
+int current_device() {
+  int d = 0;
+  return cudaGetDevice(&d) == cudaSuccess && d >= 0 && d < kMaxDevices ? d : -1;
 }
 
 }  // namespace
+
+const WorldTrig* world_trig() {
+  const int d = current_device();
+  if (d < 0) return nullptr;
+  std::lock_guard<std::mutex> lock(g_trig_mu);
+  return g_trig[d].dev;
+}
+
+void register_world_seed(int ws, cudaStream_t stream) {
+  const int d = current_device();
+  if (d < 0) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (cs != cudaStreamCaptureStatusNone) return;  // no allocation or copy inside a capture
+  std::lock_guard<std::mutex> lock(g_trig_mu);
+  TrigRegistry& r = g_trig[d];
+  for (int i = 0; i < r.used; i++)
+    if (r.seeds[i] == ws) return;
+  if (r.used == kTrigSlots) return;  // full: later seeds keep make_instance's values
+  if (r.dev == nullptr) {
+    if (cudaMalloc(&r.dev, sizeof(WorldTrig) * kTrigSlots) != cudaSuccess) {
+      cudaGetLastError();
+      r.dev = nullptr;
+      return;
+    }
+    if (cudaMemset(r.dev, 0, sizeof(WorldTrig) * kTrigSlots) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(r.dev);
+      r.dev = nullptr;
+      return;
+    }
+  }
+  // The harness's values: yaw as forestYaw computes it (float arithmetic,
+  // Arbor.cu:66), then the C library's cosf/sinf of -yaw and yaw
+  // (Arbor.cu:67-69).
+  static WorldTrig slot;
+  slot.ws = ws;
+  slot.ready = 0;
+  for (int t = 0; t < kForest; t++) {
+    const float yaw = forest_yaw(t, ws);
+    const float a = -yaw;
+    slot.v[t] = make_float4(::cosf(a), ::sinf(a), ::cosf(yaw), ::sinf(yaw));
+  }
+  WorldTrig* dst = r.dev + r.used;
+  const int header[2] = {ws, 1};
+  if (cudaMemcpyAsync(dst->v, slot.v, sizeof(slot.v), cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess ||
+      cudaMemcpyAsync(dst, header, sizeof(header), cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  r.seeds[r.used++] = ws;
+}
+
 }  // namespace arbor
 
 using namespace arbor;
@@ -131,7 +210,8 @@ extern "C" int arbor_forestInstances(int world_seed, float* instances, arbor_str
   static_assert(sizeof(Instance) == ARBOR_INSTANCE_FLOATS * 4, "Instance record layout");
   const Binding b[] = {{instances, (size_t)kForest * sizeof(Instance), true, 16, "instances"}};
   if (int s = check_bindings("arbor_forestInstances", b)) return s;
-  forest_instances_kernel<<<(kForest + 127) / 128, 128, 0, stream>>>(reinterpret_cast<Instance*>(instances), world_seed);
+  register_world_seed(world_seed, stream);
+  forest_instances_kernel<<<(kForest + 127) / 128, 128, 0, stream>>>(reinterpret_cast<Instance*>(instances), world_seed, world_trig());
   count_launch();
   return check_launch("arbor_forestInstances");
 }
@@ -151,6 +231,7 @@ extern "C" int arbor_setSample(float* C, int sample, int reset, arbor_stream str
 extern "C" int arbor_initCamera(float* C, const float* P, int seed, arbor_stream stream) {
   const Binding b[] = {{C, kC, true, 4, "C"}, {P, kP, false, 4, "P"}};
   if (int s = check_bindings("arbor_initCamera", b)) return s;
+  register_world_seed(seed, stream);
   init_camera_kernel<<<1, 1, 0, stream>>>(C, seed);
   count_launch();
   return check_launch("arbor_initCamera");

@@ -27,10 +27,11 @@ namespace {
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock) trace_work_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                             const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                            const WorldTrig* __restrict__ trig,
                                                             int width, int height) {
   __shared__ Camera cam;
   __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
+  block_setup(C, cam, inst, kForestScene, trig);
   int x, y;
   tile_pixel(threadIdx.x, x, y);
   if (x >= width || y >= height) return;
@@ -56,10 +57,11 @@ __global__ void __launch_bounds__(kBlock) trace_work_kernel(const float* __restr
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock) shade_work_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                             const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                            const WorldTrig* __restrict__ trig,
                                                             const float* __restrict__ Hit, int width, int height) {
   __shared__ Camera cam;
   __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
+  block_setup(C, cam, inst, kForestScene, trig);
   int x, y;
   tile_pixel(threadIdx.x, x, y);
   if (x >= width || y >= height) return;
@@ -106,9 +108,9 @@ extern "C" int arbor_traceWork(const float* P, const float* Nodes, const uint32_
   if (cudaMemcpyToSymbolAsync(g_work_slots, &slots, sizeof(slots), 0, cudaMemcpyHostToDevice, stream) != cudaSuccess) return check_launch(name);
   dim3 grid((width + kTile - 1) / kTile, (height + kTile - 1) / kTile);
   if (single_tree)
-    trace_work_kernel<false><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, width, height);
+    trace_work_kernel<false><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), width, height);
   else
-    trace_work_kernel<true><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, width, height);
+    trace_work_kernel<true><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), width, height);
   count_launch();
   return check_launch(name);
 }
@@ -131,9 +133,9 @@ extern "C" int arbor_shadeWork(const float* P, const float* Nodes, const uint32_
   if (cudaMemcpyToSymbolAsync(g_work_slots, &slots, sizeof(slots), 0, cudaMemcpyHostToDevice, stream) != cudaSuccess) return check_launch(name);
   dim3 grid((width + kTile - 1) / kTile, (height + kTile - 1) / kTile);
   if (single_tree)
-    shade_work_kernel<false><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    shade_work_kernel<false><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), Hit, width, height);
   else
-    shade_work_kernel<true><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    shade_work_kernel<true><<<grid, kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), Hit, width, height);
   count_launch();
   return check_launch(name);
 }

@@ -797,9 +797,10 @@ __global__ void features_kernel(const float4* __restrict__ lin, const float4* __
   }
 }
 
-// L1 loss in log(1 + radiance): prediction = log(1 + base) + out[0:3].
+// Loss in log(1 + radiance), prediction = log(1 + base) + out[0:3]: mean
+// absolute difference (l2 = false) or mean squared difference (l2 = true).
 __global__ void loss_kernel(const float* __restrict__ out, const float4* __restrict__ noisy, const float4* __restrict__ target,
-                            bf16* __restrict__ dout, float* __restrict__ loss, long pixels, float scale) {
+                            bf16* __restrict__ dout, float* __restrict__ loss, long pixels, float scale, bool l2) {
   __shared__ float part[256];
   float s = 0.0f;
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += (long)gridDim.x * blockDim.x) {
@@ -810,8 +811,13 @@ __global__ void loss_kernel(const float* __restrict__ out, const float4* __restr
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const float diff = log1pf(fmaxf(nv[c], 0.0f)) + out[p * kOutC + c] - log1pf(fmaxf(tv[c], 0.0f));
-      s += fabsf(diff);
-      g[c] = diff > 0.0f ? scale : (diff < 0.0f ? -scale : 0.0f);
+      if (l2) {
+        s += diff * diff;
+        g[c] = 2.0f * scale * diff;
+      } else {
+        s += fabsf(diff);
+        g[c] = diff > 0.0f ? scale : (diff < 0.0f ? -scale : 0.0f);
+      }
     }
 #pragma unroll
     for (int k = 0; k < kOutC / 2; k++) d[k] = __floats2bfloat162_rn(g[2 * k], g[2 * k + 1]);
@@ -966,6 +972,7 @@ struct arbor_denoiser {
   float* part = nullptr;  // partial weight / bias gradients of one layer (wgrad_kernel, bgrad_kernel)
   size_t part_floats = 0;
   bool tc = true;         // forward convolutions on tcgen05
+  bool l2 = false;        // training loss: squared (true) or absolute (false) difference in log(1 + radiance)
   long steps = 0;
   size_t allocated = 0;
 };
@@ -1383,6 +1390,16 @@ extern "C" int arbor_denoiser_set_backend(arbor_denoiser* d, int tcgen05) {
   return ARBOR_OK;
 }
 
+extern "C" int arbor_denoiser_set_loss(arbor_denoiser* d, int kind) {
+  if (int s = live(d, "arbor_denoiser_set_loss")) return s;
+  if (kind != ARBOR_LOSS_L1 && kind != ARBOR_LOSS_L2) {
+    set_error("arbor_denoiser_set_loss: kind must be ARBOR_LOSS_L1 (0) or ARBOR_LOSS_L2 (1), got %d", kind);
+    return ARBOR_ERR_VALUE;
+  }
+  d->l2 = kind == ARBOR_LOSS_L2;
+  return ARBOR_OK;
+}
+
 extern "C" int arbor_denoiser_param_count(arbor_denoiser* d, size_t* count) {
   if (int s = live(d, "arbor_denoiser_param_count")) return s;
   if (count == nullptr) {
@@ -1460,7 +1477,7 @@ extern "C" int arbor_denoiser_train_step(arbor_denoiser* d, const uint16_t* feat
   const long px = (long)batch * width * height;
   DN_CUDA(cudaMemsetAsync(d->loss, 0, 4, s));
   loss_kernel<<<ew_grid(px), 256, 0, s>>>(d->out, reinterpret_cast<const float4*>(base), reinterpret_cast<const float4*>(target), d->dout,
-                                          d->loss, px, 1.0f / (float)(px * 3));
+                                          d->loss, px, 1.0f / (float)(px * 3), d->l2);
   count_launch();
   if (int st = check_launch("loss_kernel")) return st;
   if (int st = backward(d, f, batch, width, height)) return st;
@@ -1498,7 +1515,7 @@ extern "C" int arbor_denoiser_gradient(arbor_denoiser* d, const uint16_t* featur
   const long px = (long)batch * width * height;
   DN_CUDA(cudaMemsetAsync(d->loss, 0, 4, s));
   loss_kernel<<<ew_grid(px), 256, 0, s>>>(d->out, reinterpret_cast<const float4*>(base), reinterpret_cast<const float4*>(target), d->dout,
-                                          d->loss, px, 1.0f / (float)(px * 3));
+                                          d->loss, px, 1.0f / (float)(px * 3), d->l2);
   count_launch();
   if (int st = check_launch("loss_kernel")) return st;
   if (int st = backward(d, f, batch, width, height)) return st;

@@ -23,6 +23,7 @@ namespace {
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock, 2) trace_pool_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                                const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                               const WorldTrig* __restrict__ trig,
                                                                float* __restrict__ Hit, int width, int height) {
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
@@ -30,7 +31,7 @@ __global__ void __launch_bounds__(kBlock, 2) trace_pool_kernel(const float* __re
   __shared__ Instance inst[kForestScene ? kForest : 1];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, kForestScene);
+  block_setup(C, cam, inst, kForestScene, trig);
   const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, kForestScene};
   const int bx = (width + 7) / 8;
   const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
@@ -43,6 +44,7 @@ __global__ void __launch_bounds__(kBlock, 2) trace_pool_kernel(const float* __re
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock, 2) shadow_pool_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                                 const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                                const WorldTrig* __restrict__ trig,
                                                                 const float* __restrict__ Guide, float* __restrict__ Linear, int width, int height) {
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
@@ -50,7 +52,7 @@ __global__ void __launch_bounds__(kBlock, 2) shadow_pool_kernel(const float* __r
   __shared__ Instance inst[kForestScene ? kForest : 1];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, kForestScene);
+  block_setup(C, cam, inst, kForestScene, trig);
   if (!(cam.shadows > 0.5f)) return;
   const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
   const int bx = (width + 7) / 8;
@@ -64,7 +66,7 @@ __global__ void __launch_bounds__(kBlock, 2) shadow_pool_kernel(const float* __r
 __global__ void __launch_bounds__(kBlock) shadow_setup_kernel(const float* __restrict__ C, const float* __restrict__ Hit, float* __restrict__ Linear,
                                                               float* __restrict__ Guide, int width, int height) {
   __shared__ Camera cam;
-  block_setup(C, cam, nullptr, false);
+  block_setup(C, cam, nullptr, false, nullptr);
   if (!(cam.shadows > 0.5f)) return;
   int x, y;
   tile_pixel_at(threadIdx.x, blockIdx.x * kTile, blockIdx.y * kTile, kTile, x, y);
@@ -75,12 +77,13 @@ __global__ void __launch_bounds__(kBlock) shadow_setup_kernel(const float* __res
 // with the shadow pass's visibility; 4 CTAs per SM (64 registers) hide its
 // memory latency better than 3 (measured 0.557 -> 0.530 ms at 1080p).
 template <bool kForestScene>
-__global__ void __launch_bounds__(kBlock, 4) shade_compose_kernel(const float* __restrict__ P, const float* __restrict__ C, const float* __restrict__ Hit,
-                                                               float* __restrict__ Linear, float* __restrict__ Guide, float* __restrict__ Normal,
-                                                               int width, int height) {
+__global__ void __launch_bounds__(kBlock, 4) shade_compose_kernel(const float* __restrict__ P, const float* __restrict__ C,
+                                                                  const WorldTrig* __restrict__ trig, const float* __restrict__ Hit,
+                                                                  float* __restrict__ Linear, float* __restrict__ Guide, float* __restrict__ Normal,
+                                                                  int width, int height) {
   __shared__ Camera cam;
   __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
+  block_setup(C, cam, inst, kForestScene, trig);
   int x, y;
   tile_pixel_at(threadIdx.x, blockIdx.x * kTile, blockIdx.y * kTile, kTile, x, y);
   if (x < width && y < height) shade_compose_px<kForestScene>(P, cam, inst, Hit, Linear, Guide, Normal, x, y, width, height);
@@ -105,6 +108,7 @@ __device__ __forceinline__ void species_setup(Instance* inst, const SpeciesMap& 
 
 __global__ void __launch_bounds__(kBlock, 2) trace_species_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                                   const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                                  const WorldTrig* __restrict__ trig,
                                                                   float* __restrict__ Hit, int width, int height, const SpeciesMap map) {
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
@@ -112,7 +116,7 @@ __global__ void __launch_bounds__(kBlock, 2) trace_species_kernel(const float* _
   __shared__ Instance inst[kForest];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, true);
+  block_setup(C, cam, inst, true, trig);
   species_setup(inst, map);
   const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, true, true};
   const int bx = (width + 7) / 8;
@@ -122,6 +126,7 @@ __global__ void __launch_bounds__(kBlock, 2) trace_species_kernel(const float* _
 
 __global__ void __launch_bounds__(kBlock, 2) shadow_species_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                                    const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                                   const WorldTrig* __restrict__ trig,
                                                                    const float* __restrict__ Guide, float* __restrict__ Linear, int width, int height,
                                                                    const SpeciesMap map) {
   extern __shared__ float4 batch_smem[];
@@ -130,7 +135,7 @@ __global__ void __launch_bounds__(kBlock, 2) shadow_species_kernel(const float* 
   __shared__ Instance inst[kForest];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, true);
+  block_setup(C, cam, inst, true, trig);
   if (!(cam.shadows > 0.5f)) return;
   species_setup(inst, map);
   const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, true, true};
@@ -140,11 +145,12 @@ __global__ void __launch_bounds__(kBlock, 2) shadow_species_kernel(const float* 
 }
 
 __global__ void __launch_bounds__(kBlock, 4) shade_compose_species_kernel(const float* __restrict__ P, const float* __restrict__ C,
+                                                                          const WorldTrig* __restrict__ trig,
                                                                           const float* __restrict__ Hit, float* __restrict__ Linear,
                                                                           float* __restrict__ Guide, int width, int height, const SpeciesMap map) {
   __shared__ Camera cam;
   __shared__ Instance inst[kForest];
-  block_setup(C, cam, inst, true);
+  block_setup(C, cam, inst, true, trig);
   species_setup(inst, map);
   int x, y;
   tile_pixel_at(threadIdx.x, blockIdx.x * kTile, blockIdx.y * kTile, kTile, x, y);
@@ -159,10 +165,11 @@ __global__ void __launch_bounds__(kBlock, 4) shade_compose_species_kernel(const 
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock) trace_inorder_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                                const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                               const WorldTrig* __restrict__ trig,
                                                                float* __restrict__ Hit, int width, int height) {
   __shared__ Camera cam;
   __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
+  block_setup(C, cam, inst, kForestScene, trig);
   int x, y;
   tile_pixel(threadIdx.x, x, y);
   if (x >= width || y >= height) return;
@@ -180,11 +187,12 @@ __global__ void __launch_bounds__(kBlock) trace_inorder_kernel(const float* __re
 template <bool kForestScene>
 __global__ void __launch_bounds__(kBlock) shade_inorder_kernel(const float* __restrict__ P, const float* __restrict__ Nodes,
                                                                const uint32_t* __restrict__ Order, const float* __restrict__ C,
+                                                               const WorldTrig* __restrict__ trig,
                                                                const float* __restrict__ Hit, float* __restrict__ Linear,
                                                                float* __restrict__ Guide, int width, int height) {
   __shared__ Camera cam;
   __shared__ Instance inst[kForestScene ? kForest : 1];
-  block_setup(C, cam, inst, kForestScene);
+  block_setup(C, cam, inst, kForestScene, trig);
   int x, y;
   tile_pixel(threadIdx.x, x, y);
   if (x >= width || y >= height) return;
@@ -305,9 +313,9 @@ int trace_entry(const char* name, bool forest, const float* P, const float* Node
     return ARBOR_ERR_CUDA;
   }
   if (forest)
-    trace_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, world_trig(), Hit, width, height);
   else
-    trace_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, world_trig(), Hit, width, height);
   count_launch();
   return check_launch(name);
 }
@@ -335,11 +343,11 @@ int shade_entry(const char* name, bool forest, const float* P, const float* Node
   // (its code stays small), then the shading of every pixel.
   shadow_setup_kernel<<<pixel_grid(width, height), kBlock, 0, stream>>>(C, Hit, Linear, Guide, width, height);
   if (forest) {
-    shadow_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Guide, Linear, width, height);
-    shade_compose_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, Normal, width, height);
+    shadow_pool_kernel<true><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, world_trig(), Guide, Linear, width, height);
+    shade_compose_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, world_trig(), Hit, Linear, Guide, Normal, width, height);
   } else {
-    shadow_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Guide, Linear, width, height);
-    shade_compose_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, Normal, width, height);
+    shadow_pool_kernel<false><<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, world_trig(), Guide, Linear, width, height);
+    shade_compose_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, world_trig(), Hit, Linear, Guide, Normal, width, height);
   }
   count_launch(3);
   return check_launch(name);
@@ -390,7 +398,7 @@ extern "C" int arbor_traceSpeciesPixels(const float* P, const float* Nodes, cons
     set_error("%s: cannot reserve %zu bytes of shared memory per CTA", name, kBatchSmem);
     return ARBOR_ERR_CUDA;
   }
-  trace_species_kernel<<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Hit, width, height, map);
+  trace_species_kernel<<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, world_trig(), Hit, width, height, map);
   count_launch();
   return check_launch(name);
 }
@@ -413,8 +421,8 @@ extern "C" int arbor_shadeSpeciesPixels(const float* P, const float* Nodes, cons
     return ARBOR_ERR_CUDA;
   }
   shadow_setup_kernel<<<pixel_grid(width, height), kBlock, 0, stream>>>(C, Hit, Linear, Guide, width, height);
-  shadow_species_kernel<<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, Guide, Linear, width, height, map);
-  shade_compose_species_kernel<<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, Hit, Linear, Guide, width, height, map);
+  shadow_species_kernel<<<pool_grid(width, height), kBlock, kBatchSmem, stream>>>(P, Nodes, Order, C, world_trig(), Guide, Linear, width, height, map);
+  shade_compose_species_kernel<<<pixel_grid(width, height), kBlock, 0, stream>>>(P, C, world_trig(), Hit, Linear, Guide, width, height, map);
   count_launch(3);
   return check_launch(name);
 }
@@ -456,9 +464,9 @@ extern "C" int arbor_tracePixelsInOrder(const float* P, const float* Nodes, cons
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
   if (single_tree)
-    trace_inorder_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_inorder_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), Hit, width, height);
   else
-    trace_inorder_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, width, height);
+    trace_inorder_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), Hit, width, height);
   count_launch();
   return check_launch(name);
 }
@@ -474,9 +482,9 @@ extern "C" int arbor_shadePixelsInOrder(const float* P, const float* Nodes, cons
   if (int s = check_bindings(name, b)) return s;
   if (empty) return ARBOR_OK;
   if (single_tree)
-    shade_inorder_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+    shade_inorder_kernel<false><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), Hit, Linear, Guide, width, height);
   else
-    shade_inorder_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, Hit, Linear, Guide, width, height);
+    shade_inorder_kernel<true><<<pixel_grid(width, height), kBlock, 0, stream>>>(P, Nodes, Order, C, world_trig(), Hit, Linear, Guide, width, height);
   count_launch();
   return check_launch(name);
 }

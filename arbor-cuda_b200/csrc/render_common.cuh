@@ -47,12 +47,15 @@ __device__ __forceinline__ void tile_pixel(int t, int& x, int& y) {
   x = blockIdx.x * kTile + (warp & 1) * 8 + (lane & 7);
   y = blockIdx.y * kTile + (warp >> 1) * 4 + (lane >> 3);
 }
-// Block prologue: camera constants and (forest scenes) the instance table.
-__device__ __forceinline__ void block_setup(const float* C, Camera& cam, Instance* inst, bool forest) {
+// Block prologue: camera constants and (forest scenes) the instance table,
+// its yaw sines and cosines from the world-seed registry `trig` where it has
+// the scene's seed.
+__device__ __forceinline__ void block_setup(const float* C, Camera& cam, Instance* inst, bool forest, const WorldTrig* trig) {
   if (threadIdx.x == 0) load_camera(C, cam);
   if (forest) {
-    int ws = (int)C[31];
-    for (int t = threadIdx.x; t < kForest; t += blockDim.x) inst[t] = make_instance(t, ws);
+    const int ws = (int)C[31];
+    const float4* yaw_trig = world_trig_of(trig, ws);
+    for (int t = threadIdx.x; t < kForest; t += blockDim.x) inst[t] = make_instance(t, ws, yaw_trig);
   }
   __syncthreads();
 }

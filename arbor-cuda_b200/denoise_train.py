@@ -124,6 +124,20 @@ def render_pair(fr: Frame, scene: Scene, C: np.ndarray, spp: int, eval_baselines
     return out
 
 
+def render_pairs(frames: list[Frame], jobs: list[tuple[Scene, np.ndarray]], spp: int, eval_baselines: bool) -> list[dict]:
+    """render_pair for many views, len(frames) at a time, view k of a group
+    on CUDA stream k: a small view's persistent passes leave SMs idle at
+    their tails, which the other streams' views fill."""
+    streams = [torch.cuda.Stream() for _ in frames]
+    out = []
+    for g in range(0, len(jobs), len(frames)):
+        for k, (scene, C) in enumerate(jobs[g:g + len(frames)]):
+            with torch.cuda.stream(streams[k]):
+                out.append(render_pair(frames[k], scene, C, spp, eval_baselines))
+        torch.cuda.synchronize()
+    return out
+
+
 def tonemap(lin: torch.Tensor, w: int, h: int, exposure: float) -> torch.Tensor:
     """resolvePixels' float colour before quantisation (Arbor.cu:303-304)."""
     c = lin.view(h, w, 4)[..., :3].double() * exposure

@@ -38,6 +38,11 @@ def forest_seed(tree: int, ws: int) -> int:
     return hash_u((tree * 92821 + ws * 68917 + 17) & 0xFFFFFFFF) & 1048575
 
 
+def forest_yaw(tree: int, ws: int) -> float:
+    """forestYaw (Arbor.cu:66): rnd(4, forestSeed) * pi * 2 in float32."""
+    return float(np.float32(np.float32(rnd(4, forest_seed(tree, ws))) * np.float32(3.14159265359)) * np.float32(2.0))
+
+
 def species_of(n_species: int, ws: int = FOREST_SEED) -> np.ndarray:
     """Species of each of the 324 instances in a forest of n_species species:
     forestSeed(t, ws) mod n_species (a seeded, roughly even split)."""

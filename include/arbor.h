@@ -421,6 +421,11 @@ ARBOR_API int arbor_denoiser_gradient(arbor_denoiser* d, const uint16_t* feature
 ARBOR_API int arbor_denoiser_infer(arbor_denoiser* d, const uint16_t* features, const float* base, float* denoised, int width, int height);
 /* Forward convolutions on tcgen05 (1, the default) or on mma.sync (0). */
 ARBOR_API int arbor_denoiser_set_backend(arbor_denoiser* d, int tcgen05);
+/* Training loss in log(1 + radiance): mean absolute difference
+ * (ARBOR_LOSS_L1, the default) or mean squared difference (ARBOR_LOSS_L2). */
+#define ARBOR_LOSS_L1 0
+#define ARBOR_LOSS_L2 1
+ARBOR_API int arbor_denoiser_set_loss(arbor_denoiser* d, int kind);
 /* Waits for the stream and reports ARBOR_ERR_TIMEOUT if a tensor-core
  * convolution gave up waiting for its MMAs since the last check. */
 ARBOR_API int arbor_denoiser_check(arbor_denoiser* d);

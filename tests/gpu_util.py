@@ -100,3 +100,12 @@ def dev_array(ptr: int, n: int, dtype=np.float32) -> np.ndarray:
     out = np.empty(n, dtype)
     assert _cudart().cudaMemcpy(out.ctypes.data, ptr, n * 4, 2) == 0  # cudaMemcpyDeviceToHost
     return out
+
+
+def dev_bits(ptr: int, n: int) -> torch.Tensor:
+    """Copy n 4-byte elements at a library-owned device address into a new
+    int32 device tensor (the bit patterns, for exact comparison on the GPU)."""
+    torch.cuda.synchronize()
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    assert _cudart().cudaMemcpy(out.data_ptr(), ptr, n * 4, 3) == 0  # cudaMemcpyDeviceToDevice
+    return out

@@ -10,6 +10,9 @@ buffers and camera record):
     of pixels: the warp batch then groups different rays, which changes only
     the order in which exactly equal hit distances are met.
 One view is also checked against the CPU oracle with the render tests' bars.
+The benchmark's own batch (64 views of 16 forests at four resolutions) is
+held to the same rules: every view bit-identical to the single-image entries,
+and one view of each resolution against the oracle on a band of rows.
 """
 import ctypes
 
@@ -75,8 +78,9 @@ class Batch:
         self.lib.arbor_batch_destroy(self.h)
 
 
-def single_image(cuda, gu, batch, v):
-    """The view rendered by the single-image entries on the batch's own scene buffers."""
+def single_image_device(cuda, gu, batch, v) -> dict:
+    """The view rendered by the single-image entries on the batch's own scene
+    buffers, left on the device."""
     _, w, h, C = batch.views[v]
     b = batch.buffers(v)
     dC = gu.dev(C)
@@ -85,6 +89,12 @@ def single_image(cuda, gu, batch, v):
     gu.ok(cuda.call("arbor_shadePixels", b.P, b.Nodes, b.Order, dC, bufs["Hit"], bufs["Linear"], bufs["Guide"], w, h))
     gu.ok(cuda.call("arbor_filterResolve", bufs["Linear"], bufs["Guide"], bufs["Hit"], bufs["Filtered"], bufs["History"], bufs["Pixels"],
                     dC, w, h))
+    return bufs
+
+
+def single_image(cuda, gu, batch, v):
+    """The view rendered by the single-image entries, copied to the host."""
+    bufs = single_image_device(cuda, gu, batch, v)
     return {k: gu.host(t, np.uint32 if k == "Pixels" else None) for k, t in bufs.items()}
 
 
@@ -217,3 +227,106 @@ def test_batch_rejections(cuda):
     px = np.zeros(10, np.uint32)
     assert lib.arbor_batch_read_pixels(h, px.ctypes.data_as(ctypes.c_void_p), px.size) == ab.ERR_LIMIT
     assert lib.arbor_batch_destroy(h) == ab.OK
+
+
+# ------------------------------------------------- the 64-view benchmark batch --
+# The benchmark's batch: 64 seeded views of 16 resident forests (master seed 7
+# and 15 drawn from it) at 320x180, 640x360, 1280x720 and 1920x1080, sun
+# shadows on, as workloads.batch_views lays them out.
+BIG_VIEWS = 64
+BIG_SCENES = 16
+
+
+@pytest.fixture(scope="module")
+def batch64(cuda):
+    seeds = workloads.batch_seeds(BIG_SCENES)
+    b = Batch(workloads.batch_views(BIG_VIEWS, seeds), seeds)
+    b.seeds = seeds
+    yield b
+    b.close()
+
+
+def test_batch_64_views_equal_single_image_entries(cuda, gu, batch64):
+    """Every view of the 64-view mixed-resolution batch, rendered in one graph
+    launch, is bit-identical in Hit, Linear, Guide, Filtered, History and
+    Pixels to the single-image entries on the same scene buffers."""
+    import torch
+
+    batch64.configure(16, 2, 0, 8)
+    batch64.call("arbor_batch_render")
+    pixels = 0
+    for v in range(len(batch64.views)):
+        _, w, h, _ = batch64.views[v]
+        b = batch64.buffers(v)
+        want = single_image_device(cuda, gu, batch64, v)
+        for k in IMAGES + ("Pixels",):
+            n = w * h * (1 if k == "Pixels" else 4)
+            assert torch.equal(gu.dev_bits(getattr(b, k), n), want[k].view(torch.int32)), f"view {v} ({w}x{h}) {k}"
+        pixels += w * h
+        del want
+    print(f"[batch 64 views] {pixels} pixels bit-identical to the single-image entries")
+    assert pixels == sum(w * h for _, w, h, _ in batch64.views)
+
+
+def first_view_of_each_size(views) -> list[int]:
+    first = {}
+    for v, (_, w, h, _) in enumerate(views):
+        first.setdefault((w, h), v)
+    return sorted(first.values())
+
+
+def test_batch_64_view_bands_against_oracle(cuda, gu, oracle, scenes, batch64):
+    """One view of each resolution of the 64-view batch against the oracle on
+    a band of 24 rows through the image centre: trace and shade on the band,
+    filter and resolve on its 20 interior rows (the filter reads 2 rows either
+    side).  Bars: IDs on >= 99.9 % of band pixels, Linear within 2e-3 on
+    >= 99.5 %, Filtered within 2e-3 and Pixels within one byte on >= 99 % of
+    interior pixels."""
+    batch64.configure(16, 2, 0, 8)
+    batch64.call("arbor_batch_render")
+    for v in first_view_of_each_size(batch64.views):
+        scene, w, h, C = batch64.views[v]
+        y0, y1 = h // 2 - 12, h // 2 + 12
+        sc = scenes(batch64.seeds[scene])
+        Hit = oracle.trace(sc, C.copy(), w, h, y0, y1)
+        Linear, Guide = oracle.shade(sc, C.copy(), Hit, w, h, y0, y1)
+        Filtered = oracle.filter(Linear, Guide, Hit, C.copy(), w, h, y0 + 2, y1 - 2)
+        Pixels = oracle.resolve(Filtered, np.zeros(w * h * 4, np.float32), C.copy(), w, h, y0 + 2, y1 - 2)
+        got = batch64.images(v)
+        band, inner = slice(y0 * w, y1 * w), slice((y0 + 2) * w, (y1 - 2) * w)
+        g, r = got["Hit"].reshape(-1, 4)[band], Hit.reshape(-1, 4)[band]
+        agree = float(np.mean((g[:, 1] == r[:, 1]) & (g[:, 2] == r[:, 2])))
+        errL = gu.rel_err(got["Linear"].reshape(-1, 4)[band, :3], Linear.reshape(-1, 4)[band, :3]).max(1)
+        errF = gu.rel_err(got["Filtered"].reshape(-1, 4)[inner, :3], Filtered.reshape(-1, 4)[inner, :3]).max(1)
+        pg = got["Pixels"][inner].view(np.uint8).reshape(-1, 4).astype(int)
+        pr = Pixels.view(np.uint8).reshape(-1, 4)[inner].astype(int)
+        bytes_ok = float(np.mean(np.abs(pg - pr).max(1) <= 1))
+        print(f"[batch 64 view {v}: {w}x{h}, scene seed {batch64.seeds[scene]}] id agreement {agree:.5f}; "
+              f"Linear within 2e-3 {np.mean(errL <= 2e-3):.5f}; Filtered {np.mean(errF <= 2e-3):.5f}; Pixels {bytes_ok:.5f}")
+        assert np.mean(r[:, 1] >= 0) > 0.05, f"view {v}: the band should hit trees"
+        assert agree >= 0.999
+        assert np.mean(errL <= 2e-3) >= 0.995
+        assert np.mean(errF <= 2e-3) >= 0.99
+        assert bytes_ok >= 0.99
+
+
+def test_batch_64_views_hit_ids_against_oracle(cuda, gu, oracle, scenes, batch64):
+    """Every view of the 64-view batch against the oracle's trace on 8 rows
+    through its centre: hit IDs agree on >= 99.9 % of all these pixels and
+    on >= 99.5 % of each view's (a view's 8 rows hold 2,560 to 15,360
+    pixels, so a handful of silhouette pixels is a per-mille)."""
+    batch64.configure(16, 2, 0, 8)
+    batch64.call("arbor_batch_render")
+    differ = total = 0
+    worst = (1.0, -1)
+    for v, (scene, w, h, C) in enumerate(batch64.views):
+        y0, y1 = h // 2 - 4, h // 2 + 4
+        ref = oracle.trace(scenes(batch64.seeds[scene]), C.copy(), w, h, y0, y1).reshape(-1, 4)[y0 * w:y1 * w]
+        got = dev_array(batch64.buffers(v).Hit + y0 * w * 16, (y1 - y0) * w * 4).reshape(-1, 4)
+        d = int(np.count_nonzero((got[:, 1] != ref[:, 1]) | (got[:, 2] != ref[:, 2])))
+        differ += d
+        total += len(ref)
+        worst = min(worst, (1.0 - d / len(ref), v))
+    print(f"[batch 64 views vs oracle, 8 rows each] {differ} of {total} pixels differ in hit IDs; worst view {worst[1]} at {worst[0]:.5f}")
+    assert 1.0 - differ / total >= 0.999
+    assert worst[0] >= 0.995

@@ -37,11 +37,14 @@ relative, with keys, order and BVH topology bit-exact).
 With ARBOR_REPORT_DIR set, each comparison appends one JSON line to
 $ARBOR_REPORT_DIR/parity_headline.jsonl.
 """
+import ctypes
 import json
+import math
 import os
 
 import numpy as np
 import pytest
+import torch
 
 from conftest import u32
 
@@ -151,8 +154,9 @@ def test_instance_table_and_tree_seeds_on_gpu(cuda, gu):
     """The forest instance table the trace/shade kernels use, computed on the
     GPU: per-tree seeds (forestSeed) bit-exact for all 324 trees; position,
     scale and wind phase bit-exact against the reference's values
-    (Arbor.cu:57-66); the yaw rotation's cos/sin equal the correctly rounded
-    values of the reference's yaw within 1 ulp."""
+    (Arbor.cu:57-66); the yaw rotation's cos/sin (the host C library's
+    values, checked exactly below) within 1 ulp of the correctly rounded
+    values of the reference's yaw."""
     out = gu.zeros_f(324 * 12)
     gu.ok(cuda.call("arbor_forestInstances", SEED, out))
     t = gu.host(out).reshape(324, 12)
@@ -283,3 +287,33 @@ def test_headline_frame_against_oracle(cuda, gu, oracle, oracle64, scenes, walk_
     assert got.gbuffer_same, "arbor_shadeGBuffer's Linear/Guide differ from arbor_shadePixels'"
     assert n_within >= 0.999, f"G-buffer normal within 2e-3 on only {n_within}"
     assert gpu_same_surface_ok, f"GPU t off the FP64 t where both hit the same primitive: {fp64}"
+
+
+def test_instance_yaw_trig_is_the_harness_libm(cuda):
+    """The per-tree yaw sines and cosines of the instance table are the host C
+    library's cosf/sinf of -yaw and yaw, as the reference harness evaluates
+    them (Arbor.cu:67-69 compiled for the CPU), for every tree of the 16
+    master seeds of the batch workload; the library computes them on the host
+    once per world seed.  About 3 % of the trees have a value that is not
+    the correctly rounded one."""
+    import ctypes.util
+
+    import workloads
+
+    libm = ctypes.CDLL(ctypes.util.find_library("m"))
+    for f in ("cosf", "sinf"):
+        getattr(libm, f).restype = ctypes.c_float
+        getattr(libm, f).argtypes = [ctypes.c_float]
+    not_correctly_rounded = 0
+    for ws in workloads.batch_seeds(16):
+        table = torch.zeros(324 * 12, dtype=torch.float32, device="cuda")
+        assert cuda.call("arbor_forestInstances", ws, table) == cuda.OK, cuda.last_error()
+        got = table.cpu().numpy().reshape(324, 12)[:, 5:9]
+        for t in range(324):
+            yaw = workloads.forest_yaw(t, ws)
+            a = float(np.float32(-yaw))
+            want = [libm.cosf(a), libm.sinf(a), libm.cosf(yaw), libm.sinf(yaw)]
+            assert list(got[t]) == [np.float32(x) for x in want], f"seed {ws} tree {t}"
+            exact = [np.float32(math.cos(a)), np.float32(math.sin(a)), np.float32(math.cos(yaw)), np.float32(math.sin(yaw))]
+            not_correctly_rounded += any(np.float32(x) != y for x, y in zip(want, exact))
+    print(f"[instance yaw] {not_correctly_rounded} of {16 * 324} trees have a libm value that is not correctly rounded")
