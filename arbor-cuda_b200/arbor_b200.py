@@ -26,6 +26,7 @@ STATUS = {
     5: "ARBOR_ERR_LIMIT", 6: "ARBOR_ERR_CUDA", 7: "ARBOR_ERR_TIMEOUT", 8: "ARBOR_ERR_STATE", 9: "ARBOR_ERR_NO_DEVICE",
 }
 OK, ERR_NULL, ERR_VALUE, ERR_ALIGN, ERR_ALIAS, ERR_LIMIT, ERR_CUDA, ERR_TIMEOUT, ERR_STATE, ERR_NO_DEVICE = range(10)
+LOSS_L1, LOSS_L2 = 0, 1  # arbor_denoiser_set_loss kinds
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int

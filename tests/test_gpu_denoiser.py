@@ -11,7 +11,9 @@ nearby values.  Bars: forward output within 2e-2 of its scale (max abs) and
 the update's sign equals the reference gradient's sign on >= 99% of the
 parameters whose gradient is at least 1% of the largest in their layer, and
 the gradient itself (read back without a step) has a cosine similarity of
-at least 0.997 and a relative L2 error of at most 8e-2 in every layer.
+at least 0.997 and a relative L2 error of at most 8e-2 in every layer; with
+every pre-activation positive (no leaky-ReLU kink between the two forward
+passes) at most 2e-2.
 """
 import ctypes
 
@@ -170,10 +172,11 @@ def test_first_adam_step_follows_reference_gradient(cuda):
 def test_gradient_matches_reference(cuda):
     """The backward kernels' gradient (arbor_denoiser_gradient) against the
     FP32 autograd gradient of the same loss on the same BF16 values: per
-    layer, cosine similarity >= 0.997 and relative L2 error <= 8e-2 (the
-    backward passes carry activations and output gradients in BF16; measured
-    worst layer 0.9987 and 5.2e-2 on this case); the loss within 2e-3 of the
-    reference's.  The parameters are unchanged."""
+    layer, cosine similarity >= 0.997 and relative L2 error <= 8e-2
+    (measured worst layer 0.9987 and 5.2e-2 on this case, mostly from
+    pre-activations on different sides of leaky ReLU's kink in the two
+    forward passes: test_gradient_in_the_linear_regime); the loss within
+    2e-3 of the reference's.  The parameters are unchanged."""
     batch, w, h = 2, 32, 32
     net = Net(batch, w, h, seed=5)
     try:
@@ -208,6 +211,62 @@ def test_gradient_matches_reference(cuda):
         assert abs(lval.value - loss.item()) <= 2e-3 * max(1.0, loss.item())
         assert worst_cos >= 0.997
         assert worst_rel <= 8e-2
+    finally:
+        net.close()
+
+
+def test_gradient_in_the_linear_regime(cuda):
+    """The backward kernels' arithmetic alone.  In the randomly initialised
+    network above, some pre-activations sit so close to zero that the
+    library's and the reference's forward passes (same BF16 values,
+    different FP32 summation orders) put them on different sides of leaky
+    ReLU's kink: there the two backward passes scale the gradient by 1 and
+    by 0.1.  With the library's own loss signs given to the reference the
+    error stays at 4.9 % (measured), so the kink, not the loss, is the
+    source of the 5 % allowed above.  Here
+    every pre-activation is positive by construction (biases 4, weights at
+    a fifth of He scale), so both networks are linear and every loss term's
+    sign is the same (the prediction exceeds the target by about 3 in
+    log space): per layer, relative L2 error <= 2e-2 and cosine >= 0.9998
+    (measured at most 6.1e-3)."""
+    batch, w, h = 2, 32, 32
+    net = Net(batch, w, h, seed=5)
+    try:
+        g = torch.Generator().manual_seed(9)
+        flat = []
+        for cin, cout, _ in SPEC:
+            std = 0.2 * (2.0 / (9 * cin)) ** 0.5
+            flat.append((torch.randn(cout, cin, 3, 3, generator=g) * std).permute(0, 2, 3, 1).reshape(-1))
+            flat.append(torch.full((cout,), 4.0))
+        p0 = torch.cat(flat).contiguous()
+        pn = p0.numpy()
+        assert net.lib.arbor_denoiser_set_params(net.h, pn.ctypes.data, pn.size) == ab.OK, ab.last_error()
+        layers = unpack(p0.clone())
+        feat, noisy, target = random_inputs(batch, w, h, seed=1)
+        params = [t.clone().requires_grad_(True) for pair in layers for t in pair]
+        ref_layers = [(params[2 * i], params[2 * i + 1]) for i in range(len(SPEC))]
+        out = reference_forward(ref_layers, feat.permute(0, 3, 1, 2))[:, :3].permute(0, 2, 3, 1)
+        resid = torch.log1p(noisy[..., :3].clamp(min=0)) + out - torch.log1p(target[..., :3].clamp(min=0))
+        assert bool((resid > 0.5).all()), "every loss term must keep its sign"
+        resid.abs().mean().backward()
+        gref = torch.cat([torch.cat([params[2 * i].grad.permute(0, 2, 3, 1).reshape(-1), params[2 * i + 1].grad]) for i in range(len(SPEC))])
+        grad = np.zeros(net.count, np.float32)
+        lval = ctypes.c_float()
+        fdev, ndev, tdev = to_dev_bf16(feat), noisy.contiguous().cuda(), target.contiguous().cuda()
+        st = net.lib.arbor_denoiser_gradient(net.h, fdev.data_ptr(), ndev.data_ptr(), tdev.data_ptr(), batch, w, h, grad.ctypes.data, grad.size,
+                                             ctypes.byref(lval))
+        assert st == ab.OK, ab.last_error()
+        gl = torch.from_numpy(grad)
+        off, worst_cos, worst_rel = 0, 1.0, 0.0
+        for cin, cout, _ in SPEC:
+            n = cout * 9 * cin + cout
+            a_, b_ = gl[off:off + n].double(), gref[off:off + n].double()
+            worst_cos = min(worst_cos, float((a_ @ b_) / (a_.norm() * b_.norm() + 1e-30)))
+            worst_rel = max(worst_rel, float((a_ - b_).norm() / (b_.norm() + 1e-30)))
+            off += n
+        print(f"[denoiser gradient, linear regime] worst layer cosine {worst_cos:.6f}, relative L2 error {worst_rel:.4f}")
+        assert worst_cos >= 0.9998
+        assert worst_rel <= 2e-2
     finally:
         net.close()
 
