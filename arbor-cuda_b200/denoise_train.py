@@ -3,8 +3,16 @@ GPU by the library's own kernels, and evaluation against filterLighting.
 
     python arbor-cuda_b200/denoise_train.py [--train-views 96] [--eval-views 64]
         [--size 384] [--spp 256] [--steps 1500] [--batch 4] [--lr 5e-4]
-        [--warmup 1000] [--hflip] [--loss l1|l2] [--streams 8]
+        [--warmup 1000] [--hflip] [--loss l1|l2] [--streams 8] [--crop 256]
         [--eval-width 1920 --eval-height 1080] [--eval-spp 64] [--out results.json]
+
+At the stated size (2,048 256x256 pairs' worth of 1/256-spp training pixels,
+64 held-out full-HD poses against 256-spp renders; about 35 minutes on one
+B200, most of it rendering):
+
+    python arbor-cuda_b200/denoise_train.py --train-views 512 --size 512 --crop 256 \
+        --spp 256 --eval-views 64 --eval-width 1920 --eval-height 1080 --eval-spp 256 \
+        --steps 40000 --batch 4 --lr 5e-4 --warmup 1000 --hflip --streams 8
 
 Data: views of the 324-tree forest from 16 master seeds at random poses
 (1.72 m eye height, sun shadows on), `size` x `size` pixels with the
@@ -17,7 +25,8 @@ target: the mean of Linear over `spp` samples.
 
 The network corrects filterLighting's 1-spp output (its base image) using
 the features; training minimises L1 (or L2) in log(1 + radiance) with Adam:
-each step a batch of random training views, each mirrored with probability
+each step a batch of random training views (random --crop windows of them
+when given), each mirrored with probability
 1/2 under --hflip, the learning rate ramped up over --warmup steps and then
 decayed on a cosine.  Peak rates of 1e-3 and above diverged on runs of
 20,000 steps (loss spikes, then NaN); 5e-4 with the warm-up did not.
@@ -316,7 +325,7 @@ def main() -> None:
                     "mma.sync m16n8k16 folded in a fixed order",
         "data": {"train_views": args.train_views, "eval_views": args.eval_views, "size": S, "spp_target": args.spp, "scenes": args.scenes, "hflip": bool(args.hflip), "streams": args.streams, "crop": R,
                  "eval_size": [EW, EH], "eval_spp_target": eval_spp, "render_seconds": round(t_data, 1)},
-        "train": {"steps": args.steps, "batch": args.batch, "lr": args.lr, "warmup": args.warmup, "loss": args.loss, "seconds": round(t_train, 2),
+        "train": {"steps": args.steps, "batch": args.batch, "lr": args.lr, "warmup": args.warmup, "loss_kind": args.loss, "seconds": round(t_train, 2),
                   "ms_per_step": round(1e3 * t_train / max(1, args.steps), 3), "loss": losses},
         "psnr_db_mean": mean,
         "psnr_db_min": {k: round(float(np.min(v)), 3) for k, v in scores.items()},
