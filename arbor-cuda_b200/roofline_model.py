@@ -76,11 +76,12 @@ def flops(counts: dict) -> int:
 # DRAM traffic per unit, measured with ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum) on one 960x544 launch of the forest walk's first
 # frame (seed 7, cold caches): the trace kernel moved 5.33 MB for 522,240
-# primary rays, the shadow pass of shadePixels 13.85 MB for 522,240 pixels.
+# primary rays, the shadow pass of shadePixels 20.31 MB for 522,240 pixels
+# (warp-batch queue depth 12).
 # The 5.7 MB scene stays in L2, so the traffic grows with the pixel count;
 # bench lines scale these to their launch.
 TRACE_DRAM_BYTES_PER_RAY = 10.2
-SHADOW_DRAM_BYTES_PER_PIXEL = 26.5
+SHADOW_DRAM_BYTES_PER_PIXEL = 38.9
 TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 960x544 forest launch, scaled by units to this launch"
 
 
