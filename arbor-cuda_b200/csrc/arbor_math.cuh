@@ -215,13 +215,18 @@ __device__ __forceinline__ Instance make_instance(int tree, int ws) {
 // one unit in the last place away from make_instance's correctly rounded
 // one, which turns the tree by that much and changes hit IDs along its
 // silhouettes.  The host fills a registry slot per world seed
-// (register_world_seed, camera.cu) and block prologues take the four values
-// from it; a seed without a slot keeps make_instance's values.
+// (register_world_seed, camera.cu) with these values and the whole instance
+// table built from them; block prologues take the values from it, and the
+// persistent trace and shadow passes read the slot's table in place (global
+// memory, L1/L2-resident) instead of building one in shared memory, which
+// leaves their warp batches the room for deeper queues.  A seed without a
+// slot keeps make_instance's values.
 constexpr int kTrigSlots = 64;
 struct WorldTrig {
-  int ws, ready;        // world seed; 1 once the values below are in place
+  int ws, ready;          // world seed; 1 once the values below are in place
   int pad[2];
-  float4 v[kForest];    // per tree: cos(-yaw), sin(-yaw), cos(yaw), sin(yaw)
+  float4 v[kForest];      // per tree: cos(-yaw), sin(-yaw), cos(yaw), sin(yaw)
+  Instance inst[kForest]; // make_instance(t, ws, v) of every tree
 };
 // Host: the registry of the current device (nullptr if it cannot be
 // allocated) and the registration of a world seed (a no-op for a seed already
@@ -229,9 +234,9 @@ struct WorldTrig {
 const WorldTrig* world_trig();
 void register_world_seed(int ws, cudaStream_t stream);
 
-// Block-wide: the registry's values for world seed ws, or nullptr.  Every
-// thread of the block calls it (it synchronises the block).
-__device__ __forceinline__ const float4* world_trig_of(const WorldTrig* trig, int ws) {
+// Block-wide: the registry slot of world seed ws, or nullptr.  Every thread
+// of the block calls it (it synchronises the block; blockDim.x >= 64).
+__device__ __forceinline__ const WorldTrig* world_slot_of(const WorldTrig* trig, int ws) {
   __shared__ int slot;
   if (threadIdx.x == 0) slot = -1;
   __syncthreads();
@@ -240,7 +245,12 @@ __device__ __forceinline__ const float4* world_trig_of(const WorldTrig* trig, in
     if (s->ready == 1 && s->ws == ws) atomicMax(&slot, (int)threadIdx.x);
   }
   __syncthreads();
-  return slot >= 0 ? trig[slot].v : nullptr;
+  return slot >= 0 ? trig + slot : nullptr;
+}
+// Block-wide: the registry's sines and cosines for world seed ws, or nullptr.
+__device__ __forceinline__ const float4* world_trig_of(const WorldTrig* trig, int ws) {
+  const WorldTrig* s = world_slot_of(trig, ws);
+  return s != nullptr ? s->v : nullptr;
 }
 // make_instance with the registry's sines and cosines where it has them.
 __device__ __forceinline__ Instance make_instance(int tree, int ws, const float4* yaw_trig) {

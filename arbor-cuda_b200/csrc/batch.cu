@@ -28,7 +28,7 @@
 // The autotuner times the trace, shadow and compose kernels on a sample of
 // the views for each compose tile shape (16x16 or 32x8), CTAs per SM (1 or
 // 2), view order (as given, or the largest views first) and warp-batch queue
-// depth (8 or 12 candidates per lane), and keeps the fastest.
+// depth (12 or 16 candidates per lane), and keeps the fastest.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -182,7 +182,7 @@ constexpr int kMaxScenes = 1024;
 
 bool valid_config(const arbor_batch_config& c) {
   return (c.tile_width == 16 || c.tile_width == 32) && (c.ctas_per_sm == 1 || c.ctas_per_sm == 2) && (c.order == 0 || c.order == 1) &&
-         (c.queue == 8 || c.queue == 12);
+         (c.queue == 12 || c.queue == 16);
 }
 
 }  // namespace
@@ -213,7 +213,7 @@ struct arbor_batch {
   int n_ts = 0, n_filter = 0;
   size_t tile_capacity = 0;
   void* scratch = nullptr;     // radix-sort scratch of the scene builds
-  arbor_batch_config cfg{16, 2, 0, 12};
+  arbor_batch_config cfg{16, 2, 0, 16};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t renders = 0;
@@ -253,10 +253,10 @@ int launch_setup(arbor_batch* b, cudaStream_t s) {
 int launch_trace(arbor_batch* b, const arbor_batch_config& cfg, int n_list, cudaStream_t s) {
   const dim3 grid(b->sms * cfg.ctas_per_sm);
   int* queues = b->counters + kViewQueues;
-  if (cfg.queue == 8)
-    batch_pool_kernel<8, false><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
-  else
+  if (cfg.queue == 12)
     batch_pool_kernel<12, false><<<grid, kBlock, batch_smem_bytes<12>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
+  else
+    batch_pool_kernel<16, false><<<grid, kBlock, batch_smem_bytes<16>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
   return check_launch("batch_pool_kernel");
 }
 
@@ -265,10 +265,10 @@ int launch_trace(arbor_batch* b, const arbor_batch_config& cfg, int n_list, cuda
 int launch_shade(arbor_batch* b, const arbor_batch_config& cfg, const int4* tiles, int n_tiles, int n_list, cudaStream_t s) {
   const dim3 grid(b->sms * cfg.ctas_per_sm);
   int* queues = b->counters + kViewQueues + b->n_views;
-  if (cfg.queue == 8)
-    batch_pool_kernel<8, true><<<grid, kBlock, batch_smem_bytes<8>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
-  else
+  if (cfg.queue == 12)
     batch_pool_kernel<12, true><<<grid, kBlock, batch_smem_bytes<12>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
+  else
+    batch_pool_kernel<16, true><<<grid, kBlock, batch_smem_bytes<16>(), s>>>(b->views, b->cams, b->insts, b->vlist, n_list, queues);
   if (int st = check_launch("batch_pool_kernel")) return st;
   batch_compose_kernel<<<b->sms * 8, kBlock, 0, s>>>(b->views, b->cams, b->insts, tiles, n_tiles, cfg.tile_width,
                                                      b->counters + kQueueCompose);
@@ -430,9 +430,9 @@ extern "C" int arbor_batch_create(arbor_batch** out, const int* seeds, int n_sce
   if ((ce = cudaEventCreateWithFlags(&b->joined, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_fail("cudaEventCreate", ce));
   if ((ce = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) != cudaSuccess) return fail(cuda_fail("cudaEventCreate", ce));
   {
-    const void* kernels[] = {(const void*)batch_pool_kernel<8, false>, (const void*)batch_pool_kernel<8, true>,
-                             (const void*)batch_pool_kernel<12, false>, (const void*)batch_pool_kernel<12, true>};
-    const int bytes[] = {(int)batch_smem_bytes<8>(), (int)batch_smem_bytes<8>(), (int)batch_smem_bytes<12>(), (int)batch_smem_bytes<12>()};
+    const void* kernels[] = {(const void*)batch_pool_kernel<12, false>, (const void*)batch_pool_kernel<12, true>,
+                             (const void*)batch_pool_kernel<16, false>, (const void*)batch_pool_kernel<16, true>};
+    const int bytes[] = {(int)batch_smem_bytes<12>(), (int)batch_smem_bytes<12>(), (int)batch_smem_bytes<16>(), (int)batch_smem_bytes<16>()};
     for (int k = 0; k < 4; k++)
       if ((ce = cudaFuncSetAttribute(kernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes[k])) != cudaSuccess)
         return fail(cuda_fail("cudaFuncSetAttribute", ce));
@@ -515,7 +515,7 @@ extern "C" int arbor_batch_configure(arbor_batch* b, const arbor_batch_config* c
     return ARBOR_ERR_NULL;
   }
   if (!valid_config(*cfg)) {
-    set_error("arbor_batch_configure: tile_width 16|32, ctas_per_sm 1|2, order 0|1, queue 8|12 (got %d %d %d %d)", cfg->tile_width,
+    set_error("arbor_batch_configure: tile_width 16|32, ctas_per_sm 1|2, order 0|1, queue 12|16 (got %d %d %d %d)", cfg->tile_width,
               cfg->ctas_per_sm, cfg->order, cfg->queue);
     return ARBOR_ERR_VALUE;
   }
@@ -602,7 +602,7 @@ extern "C" int arbor_batch_autotune(arbor_batch* b, int sample_views, arbor_batc
   for (int tw : {16, 32})
     for (int ctas : {1, 2})
       for (int order : {0, 1})
-        for (int q : {8, 12}) {
+        for (int q : {12, 16}) {
           const arbor_batch_config cfg{tw, ctas, order, q};
           std::vector<int4> t;
           const std::vector<int> vo = view_order(b, subset, order);

@@ -119,11 +119,18 @@ __global__ void set_sample_kernel(float* C, int sample, int reset) {
 }
 
 // The forest instance table of world seed ws, one Instance per tree: the
-// table every trace/shade CTA builds in shared memory (render_common.cuh).
+// table the trace and shade kernels use (built in shared memory by the shade
+// passes' block prologues, read from the registry by the persistent passes).
 __global__ void forest_instances_kernel(Instance* out, int ws, const WorldTrig* trig) {
   const float4* yaw_trig = world_trig_of(trig, ws);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < kForest) out[t] = make_instance(t, ws, yaw_trig);
+}
+
+// A registry slot's instance table, from the slot's own sines and cosines.
+__global__ void slot_instances_kernel(WorldTrig* slot, int ws) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < kForest) slot->inst[t] = make_instance(t, ws, slot->v);
 }
 
 // Per-device registry of world-seed yaw tables (WorldTrig).  Slots are
@@ -182,18 +189,23 @@ void register_world_seed(int ws, cudaStream_t stream) {
   // The harness's values: yaw as forestYaw computes it (float arithmetic,
   // Arbor.cu:66), then the C library's cosf/sinf of -yaw and yaw
   // (Arbor.cu:67-69).
-  static WorldTrig slot;
-  slot.ws = ws;
-  slot.ready = 0;
+  static float4 v[kForest];
   for (int t = 0; t < kForest; t++) {
     const float yaw = forest_yaw(t, ws);
     const float a = -yaw;
-    slot.v[t] = make_float4(::cosf(a), ::sinf(a), ::cosf(yaw), ::sinf(yaw));
+    v[t] = make_float4(::cosf(a), ::sinf(a), ::cosf(yaw), ::sinf(yaw));
   }
   WorldTrig* dst = r.dev + r.used;
   const int header[2] = {ws, 1};
-  if (cudaMemcpyAsync(dst->v, slot.v, sizeof(slot.v), cudaMemcpyHostToDevice, stream) != cudaSuccess ||
-      cudaStreamSynchronize(stream) != cudaSuccess ||
+  if (cudaMemcpyAsync(dst->v, v, sizeof(v), cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  // then the instance table from those values, on the device (the same
+  // make_instance as every block prologue)
+  slot_instances_kernel<<<(kForest + 127) / 128, 128, 0, stream>>>(dst, ws);
+  count_launch();
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess ||
       cudaMemcpyAsync(dst, header, sizeof(header), cudaMemcpyHostToDevice, stream) != cudaSuccess ||
       cudaStreamSynchronize(stream) != cudaSuccess) {
     cudaGetLastError();

@@ -373,7 +373,7 @@ struct ShadowPolicy {
     int id = (int)r.found;
     if (id < 0) {
       write(trans);
-    } else if (ldg4(scene_P(*ctx, ctx->species && r.foundTree >= 0 ? ctx->inst[r.foundTree].species : 0), id * 6).w != 1.0f) {
+    } else if (ldg4(scene_P(*ctx, tree_species(*ctx, r.foundTree)), id * 6).w != 1.0f) {
       write(mk(0.0f, 0.0f, 0.0f));
     } else {
       trans = trans * mk(0.18f, 0.29f, 0.065f);
@@ -427,7 +427,7 @@ struct StagedShadowPolicy {
     int id = (int)r.found;
     if (id < 0) {
       write(trans);
-    } else if (ldg4(scene_P(*ctx, ctx->species && r.foundTree >= 0 ? ctx->inst[r.foundTree].species : 0), id * 6).w != 1.0f) {
+    } else if (ldg4(scene_P(*ctx, tree_species(*ctx, r.foundTree)), id * 6).w != 1.0f) {
       write(mk(0.0f, 0.0f, 0.0f));
     } else {
       trans = trans * mk(0.18f, 0.29f, 0.065f);

@@ -17,6 +17,23 @@ namespace arbor {
 namespace {
 
 // ---------------------------------------------------------------- kernels --
+// The instance table of a persistent pass: the registry slot's (global
+// memory) when the host registered the world seed, else one built in the
+// dynamic shared memory of the CTA's last two warp batches, whose warps then
+// leave (kTableWarps warps trace).  Every thread of the block calls it.
+constexpr int kTableWarps = kBlock / 32 - 2;
+static_assert(2 * sizeof(WarpBatch) >= sizeof(Instance) * kForest, "two warp batches hold an instance table");
+__device__ __forceinline__ const Instance* pass_instances(const WorldTrig* trig, int ws, float4* smem, bool& leave) {
+  const WorldTrig* slot = world_slot_of(trig, ws);
+  leave = false;
+  if (slot != nullptr) return slot->inst;
+  Instance* table = reinterpret_cast<Instance*>(reinterpret_cast<WarpBatch*>(smem) + kTableWarps);
+  for (int t = threadIdx.x; t < kForest; t += blockDim.x) table[t] = make_instance(t, ws);
+  __syncthreads();
+  leave = (int)(threadIdx.x >> 5) >= kTableWarps;
+  return table;
+}
+
 // Persistent form of the trace: a grid of (SMs x 2) CTAs, each taking every
 // gridDim.x-th 8x4-pixel block of the image, its lanes taking pixels as
 // their rays finish (batch_run_pool).
@@ -28,10 +45,12 @@ __global__ void __launch_bounds__(kBlock, 2) trace_pool_kernel(const float* __re
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
   __shared__ Camera cam;
-  __shared__ Instance inst[kForestScene ? kForest : 1];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, kForestScene, trig);
+  block_setup(C, cam, nullptr, false, nullptr);
+  bool leave = false;
+  const Instance* inst = kForestScene ? pass_instances(trig, cam.ws, batch_smem, leave) : nullptr;
+  if (leave) return;
   const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, kForestScene};
   const int bx = (width + 7) / 8;
   const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
@@ -49,11 +68,13 @@ __global__ void __launch_bounds__(kBlock, 2) shadow_pool_kernel(const float* __r
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
   __shared__ Camera cam;
-  __shared__ Instance inst[kForestScene ? kForest : 1];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, kForestScene, trig);
+  block_setup(C, cam, nullptr, false, nullptr);
   if (!(cam.shadows > 0.5f)) return;
+  bool leave = false;
+  const Instance* inst = kForestScene ? pass_instances(trig, cam.ws, batch_smem, leave) : nullptr;
+  if (leave) return;
   const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, kForestScene};
   const int bx = (width + 7) / 8;
   const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
@@ -113,12 +134,15 @@ __global__ void __launch_bounds__(kBlock, 2) trace_species_kernel(const float* _
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
   __shared__ Camera cam;
-  __shared__ Instance inst[kForest];
+  __shared__ uint8_t of[kForest];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, true, trig);
-  species_setup(inst, map);
-  const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, true, true};
+  for (int t = threadIdx.x; t < kForest; t += blockDim.x) of[t] = map.of[t];
+  block_setup(C, cam, nullptr, false, nullptr);
+  bool leave = false;
+  const Instance* inst = pass_instances(trig, cam.ws, batch_smem, leave);
+  if (leave) return;
+  const TraceCtx c{P, Nodes, Order, inst, cam.c14 / (float)height, cam.time, cam.wind, true, true, true, of};
   const int bx = (width + 7) / 8;
   const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
   trace_pool(c, cam, b, Hit, pool);
@@ -132,13 +156,16 @@ __global__ void __launch_bounds__(kBlock, 2) shadow_species_kernel(const float* 
   extern __shared__ float4 batch_smem[];
   WarpBatch& b = reinterpret_cast<WarpBatch*>(batch_smem)[threadIdx.x >> 5];
   __shared__ Camera cam;
-  __shared__ Instance inst[kForest];
+  __shared__ uint8_t of[kForest];
   __shared__ int next;
   if (threadIdx.x == 0) next = 0;
-  block_setup(C, cam, inst, true, trig);
+  for (int t = threadIdx.x; t < kForest; t += blockDim.x) of[t] = map.of[t];
+  block_setup(C, cam, nullptr, false, nullptr);
   if (!(cam.shadows > 0.5f)) return;
-  species_setup(inst, map);
-  const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, true, true};
+  bool leave = false;
+  const Instance* inst = pass_instances(trig, cam.ws, batch_smem, leave);
+  if (leave) return;
+  const TraceCtx c{P, Nodes, Order, inst, 0.0001f, cam.time, cam.wind, false, true, true, of};
   const int bx = (width + 7) / 8;
   const PixelPool pool{&next, width, height, bx, bx * ((height + 3) / 4)};
   staged_shadow_pool(c, b, Guide, Linear, pool);

@@ -59,8 +59,16 @@ struct TraceCtx {
                           // ties settled by ref_before; false for shadow segments
   bool forest;            // false: the single-tree scene (identity instance)
   bool species = false;   // true: a forest of several species, P / Nodes / Order holding one scene
-                          // per species back to back, instance t on scene inst[t].species
+                          // per species back to back, instance t on scene species_of[t] (or
+                          // inst[t].species when species_of is null)
+  const uint8_t* species_of = nullptr;
 };
+
+// The scene of tree `tree` (0 unless the forest has several species).
+__device__ __forceinline__ int tree_species(const TraceCtx& c, int tree) {
+  if (!c.species || tree < 0) return 0;
+  return c.species_of != nullptr ? (int)c.species_of[tree] : c.inst[tree].species;
+}
 
 // The records of scene `s` (s = 0 unless the forest has several species).
 __device__ __forceinline__ const float* scene_P(const TraceCtx& c, int s) { return c.species ? c.P + (size_t)s * (kCapacity * kPS) : c.P; }
@@ -188,7 +196,7 @@ __device__ __forceinline__ void dda_step(const TraceCtx& c, Ray& r) {
     r.lbest = r.best / it.sc;
     r.ltime = c.time + it.phase;
     r.lsc = it.sc;
-    if (c.species) r.species = it.species;
+    if (c.species) r.species = tree_species(c, tree);
     if (enter_tree(c, r)) {
       r.phase = kPhTree;
       return;

@@ -31,9 +31,10 @@
 
 namespace arbor {
 
-constexpr int kQueue = 12;       // candidates a lane may queue: the most at which a 256-thread CTA's 8 warp
-                                 // batches still leave 2 CTAs per SM (12 against 8: shadow segments 10 %,
-                                 // primary rays 6 % faster on the 1080p forest walk)
+constexpr int kQueue = 16;       // candidates a lane may queue: the most at which a 256-thread CTA's 8 warp
+                                 // batches (111 KB) still leave 2 CTAs per SM, the instance table read from
+                                 // global memory (on the 1080p forest walk, shadow segments 10 % faster at
+                                 // 12 than at 8 and 5 % faster again at 16; primary rays 6 % and 4 %)
 constexpr int kNewtonCap = 64;   // pending Newton solves per warp
 enum JobClass : int { kJobLeaf = 0, kJobWood = 1, kJobMisc = 2, kJobNone = 3 };
 

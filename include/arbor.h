@@ -337,7 +337,7 @@ typedef struct arbor_batch_config {
   int tile_width;   /* shading (compose) tile: 16 (16x16 pixels) or 32 (32x8 pixels) */
   int ctas_per_sm;  /* persistent CTAs per SM: 1 or 2 */
   int order;        /* view order of every pass: 0 as given, 1 largest views first */
-  int queue;        /* warp-batch queue depth, candidates per lane: 8 or 12 */
+  int queue;        /* warp-batch queue depth, candidates per lane: 12 or 16 */
 } arbor_batch_config;
 
 typedef struct arbor_batch_info {
@@ -354,7 +354,7 @@ typedef struct arbor_batch_info {
  * view's Hit/Linear/Guide/Filtered/History/Pixels on the current device.
  * The batch works on a stream of its own, ordered after `stream` at each
  * call, and `stream` is ordered after the work each call queues.  Default
- * configuration: 16x16 tiles, 2 CTAs/SM, view order, queue depth 12 (the
+ * configuration: 16x16 tiles, 2 CTAs/SM, view order, queue depth 16 (the
  * single-image kernels' depth). */
 ARBOR_API int arbor_batch_create(arbor_batch** out, const int* seeds, int n_scenes, const arbor_batch_view* views, int n_views, arbor_stream stream);
 /* Replaces every view's camera record (n_views x 64 floats, host memory). */

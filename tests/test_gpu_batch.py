@@ -4,7 +4,7 @@ Each view of a batch must render as the single-image entries render it
 (arbor_tracePixels, arbor_shadePixels, arbor_filterResolve on the same scene
 buffers and camera record):
   - bit-identical for configurations whose warps cover the same pixels as
-    the single-image kernels (16x16 tiles, queue depth 12), whatever the CTAs
+    the single-image kernels (16x16 tiles, queue depth 16), whatever the CTAs
     per SM and the tile order;
   - for the other tile shapes and queue depths, hit IDs agree on >= 99.99%
     of pixels: the warp batch then groups different rays, which changes only
@@ -119,7 +119,7 @@ def singles(cuda, gu, batch):
 
 @pytest.mark.parametrize("ctas,order", [(2, 0), (1, 1)])
 def test_batch_equals_single_image_entries(cuda, gu, batch, singles, ctas, order):
-    batch.configure(16, ctas, order, 12)
+    batch.configure(16, ctas, order, 16)
     batch.call("arbor_batch_render")
     for v in range(len(batch.views)):
         got = batch.images(v)
@@ -127,7 +127,7 @@ def test_batch_equals_single_image_entries(cuda, gu, batch, singles, ctas, order
             assert np.array_equal(u32(got[k]), u32(singles[v][k])), f"view {v} {k}"
 
 
-@pytest.mark.parametrize("tw,queue", [(32, 12), (16, 8), (32, 8)])
+@pytest.mark.parametrize("tw,queue", [(32, 16), (16, 12), (32, 12)])
 def test_batch_other_tilings_agree(cuda, gu, batch, singles, tw, queue):
     batch.configure(tw, 2, 0, queue)
     batch.call("arbor_batch_render")
@@ -142,7 +142,7 @@ def test_batch_other_tilings_agree(cuda, gu, batch, singles, tw, queue):
 
 
 def test_batch_view_against_oracle(cuda, gu, oracle, scenes, batch):
-    batch.configure(16, 2, 0, 12)
+    batch.configure(16, 2, 0, 16)
     batch.call("arbor_batch_render")
     v = 3  # 200 x 120, seed 1788, shadows on
     scene, w, h, C = batch.views[v]
@@ -161,7 +161,7 @@ def test_batch_set_cameras_and_pixels(cuda, gu, batch, singles):
     """New cameras through arbor_batch_set_cameras render as the single-image
     path renders them; arbor_batch_read_pixels returns every view's Pixels
     back to back."""
-    batch.configure(16, 2, 0, 12)
+    batch.configure(16, 2, 0, 16)
     moved = []
     for scene, w, h, C in batch.views:
         C2 = C.copy()
@@ -198,8 +198,8 @@ def test_batch_autotune(cuda, gu, batch, singles):
     times = list(ms)
     print("[batch autotune] ms:", [round(t, 3) for t in times], "->", best.as_dict())
     assert all(t > 0 for t in times)
-    assert best.tile_width in (16, 32) and best.ctas_per_sm in (1, 2) and best.order in (0, 1) and best.queue in (8, 12)
-    k = (best.tile_width == 32) * 8 + (best.ctas_per_sm == 2) * 4 + best.order * 2 + (best.queue == 12)
+    assert best.tile_width in (16, 32) and best.ctas_per_sm in (1, 2) and best.order in (0, 1) and best.queue in (12, 16)
+    k = (best.tile_width == 32) * 8 + (best.ctas_per_sm == 2) * 4 + best.order * 2 + (best.queue == 16)
     assert times[k] == min(times)
     cur = ab.BatchConfig()
     batch.call("arbor_batch_get_config", ctypes.byref(cur))
@@ -252,7 +252,7 @@ def test_batch_64_views_equal_single_image_entries(cuda, gu, batch64):
     Pixels to the single-image entries on the same scene buffers."""
     import torch
 
-    batch64.configure(16, 2, 0, 12)
+    batch64.configure(16, 2, 0, 16)
     batch64.call("arbor_batch_render")
     pixels = 0
     for v in range(len(batch64.views)):
@@ -282,7 +282,7 @@ def test_batch_64_view_bands_against_oracle(cuda, gu, oracle, scenes, batch64):
     side).  Bars: IDs on >= 99.9 % of band pixels, Linear within 2e-3 on
     >= 99.5 %, Filtered within 2e-3 and Pixels within one byte on >= 99 % of
     interior pixels."""
-    batch64.configure(16, 2, 0, 12)
+    batch64.configure(16, 2, 0, 16)
     batch64.call("arbor_batch_render")
     for v in first_view_of_each_size(batch64.views):
         scene, w, h, C = batch64.views[v]
@@ -315,7 +315,7 @@ def test_batch_64_views_hit_ids_against_oracle(cuda, gu, oracle, scenes, batch64
     through its centre: hit IDs agree on >= 99.9 % of all these pixels and
     on >= 99.5 % of each view's (a view's 8 rows hold 2,560 to 15,360
     pixels, so a handful of silhouette pixels is a per-mille)."""
-    batch64.configure(16, 2, 0, 12)
+    batch64.configure(16, 2, 0, 16)
     batch64.call("arbor_batch_render")
     differ = total = 0
     worst = (1.0, -1)
