@@ -26,6 +26,12 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
     "-DARBOR_BUILD", "--expt-relaxed-constexpr",
 ]
+# Per-file device-assembler flags.  render.cu (the persistent trace and
+# shadow passes, the compose and filter kernels) at ptxas -O1: its warp
+# loop is bound by instruction fetch, and the less aggressively scheduled
+# code runs faster (1080p walk: trace 12.3 -> 11.9 ms, filter+resolve 66 ->
+# 64 us, compose +3 %; -O0 is 4x slower); results are bit-identical.
+FILE_FLAGS = {"render.cu": ["-Xptxas", "-O1"]}
 
 
 def nvcc() -> str:
@@ -52,7 +58,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [path, __file__] + headers):
-            cmd = [nvcc(), *NVCC_FLAGS, "-dc" if False else "-c", path, "-o", obj]
+            cmd = [nvcc(), *NVCC_FLAGS, *FILE_FLAGS.get(src, []), "-c", path, "-o", obj]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
             res = subprocess.run(cmd, capture_output=True, text=True)
