@@ -244,6 +244,17 @@ def test_walk_1080p_camera_records(oracle, scenes):
         assert np.array_equal(u32(C), u32(np.array(want, np.float32))), f"frame {frame}"
 
 
+def test_forest_yaw_helper_is_the_reference_yaw(oracle):
+    """workloads.forest_yaw (the per-tree yaw in float32, Arbor.cu:66) equals
+    the oracle's for every tree of the 16 batch seeds; the GPU tests use it
+    to recompute the C library's sines and cosines of the instance table."""
+    import workloads
+
+    for ws in workloads.batch_seeds(16):
+        for t in range(324):
+            assert np.float32(workloads.forest_yaw(t, ws)) == np.float32(oracle.forest_instance(t, ws)[4]), (ws, t)
+
+
 def test_species_forest_with_one_species_is_the_forest(oracle, scenes):
     """The forest of several species with every instance on scene 0 renders
     exactly the reference's forest (oracle_tracePixelsSpecies /
