@@ -166,7 +166,9 @@ __device__ __forceinline__ void batch_tests(const TraceCtx& c, const Ray& r, WB&
         int owner = q / WB::kQ;
         float4 o = b.rayO[owner], d = b.rayD[owner];
         float tube;
-        solve = leaf_clip(scene_P(c, c.species ? b.rayS[owner] : 0), b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls, tube);
+        const float* P = scene_P(c, c.species ? b.rayS[owner] : 0);
+        solve = c.refine ? leaf_clip_outlined(P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls, tube)
+                         : leaf_clip(P, b.prim[q], mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, c.wind, ls, tube);
         b.res[q] = tube;  // the result, or the Newton stage's starting best
       }
       unsigned m = __ballot_sync(full, solve);
