@@ -4,10 +4,11 @@
 //
 // Launch shapes: the trace and the shade's shadow pass are persistent (2
 // CTAs per SM, lanes taking pixels of 8x4 blocks as their rays finish); the
-// shade's compose pass runs 256-thread blocks over 16x16 pixel tiles.  Each
-// block builds the 324-entry forest instance table in shared memory once;
-// every table entry equals what the reference's forest helpers recompute per
-// ray (Arbor.cu:57-69).
+// shade's compose pass runs 256-thread blocks over 16x16 pixel tiles.  The
+// persistent passes read the 324-entry forest instance table from the
+// world-seed registry (pass_instances); the compose blocks build it in shared
+// memory once.  Every table entry equals what the reference's forest helpers
+// recompute per ray (Arbor.cu:57-69).
 #include <algorithm>
 
 #include "abi_util.h"

@@ -53,7 +53,7 @@ struct TraceCtx {
   const float* P;
   const float* Nodes;
   const uint32_t* Order;
-  const Instance* inst;   // forest instance table (shared memory)
+  const Instance* inst;   // forest instance table (the world-seed registry's, or shared memory)
   float cone, time, wind;
   bool refine;            // primary rays: wood refined by the SDF march, their own visiting order,
                           // ties settled by ref_before; false for shadow segments
