@@ -113,6 +113,17 @@ def test_engine_rejections_without_device(lib):
     assert lib.arbor_engine_destroy(None) == ab.OK
 
 
+def test_denoiser_rejections_without_device(lib):
+    """Null handles are rejected by every denoiser entry that takes one,
+    before any device work; the loss kinds are ARBOR_LOSS_L1 and L2."""
+    assert lib.arbor_denoiser_set_loss(None, ab.LOSS_L1) == ab.ERR_NULL
+    assert "NULL" in ab.last_error()
+    assert lib.arbor_denoiser_set_backend(None, 1) == ab.ERR_NULL
+    header = open(HEADER).read()
+    assert re.search(r"#define ARBOR_LOSS_L1 0\b", header) and re.search(r"#define ARBOR_LOSS_L2 1\b", header)
+    assert (ab.LOSS_L1, ab.LOSS_L2) == (0, 1)
+
+
 def test_launch_counter_starts_without_launches(lib):
     assert lib.arbor_launch_count() >= 0
 
