@@ -192,6 +192,31 @@ def test_port_equals_reference_walk_frames(oracle, ref, scenes):
         assert np.array_equal(u32(fa[k]), u32(fb[k])), k
 
 
+def test_port_equals_reference_on_the_batch_workload(oracle, ref):
+    """The benchmark's 64-view batch (16 master seeds, four resolutions, sun
+    shadows on): the 16 scene builds bit-identical, and trace + shade of 2
+    rows through the centre of every view bit-identical to the reference
+    harness.  The GPU batch tests compare against the port; this pins the
+    port to the reference on exactly those scenes and cameras."""
+    import workloads
+
+    seeds = workloads.batch_seeds(16)
+    built = {}
+    for k, ws in enumerate(seeds):
+        a, b = oracle.build_scene(ws), ref.build_scene(ws)
+        for key in ("B", "P", "Keys", "Order", "Nodes"):
+            assert np.array_equal(u32(a[key]), u32(b[key])), (ws, key)
+        built[k] = a
+    for v, (k, w, h, C) in enumerate(workloads.batch_views(64, seeds)):
+        y0, y1 = h // 2 - 1, h // 2 + 1
+        ha = oracle.trace(built[k], C.copy(), w, h, y0, y1)
+        hb = ref.trace(built[k], C.copy(), w, h, y0, y1)
+        assert np.array_equal(u32(ha), u32(hb)), f"view {v} Hit"
+        la, ga = oracle.shade(built[k], C.copy(), ha, w, h, y0, y1)
+        lb, gb = ref.shade(built[k], C.copy(), ha, w, h, y0, y1)
+        assert np.array_equal(u32(la), u32(lb)) and np.array_equal(u32(ga), u32(gb)), f"view {v} Linear/Guide"
+
+
 def test_f64_rerun_close_to_f32(oracle, oracle64, scenes):
     """The FP64 instantiation runs the same formulas in double.
 
