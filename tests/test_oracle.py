@@ -217,6 +217,35 @@ def test_port_equals_reference_on_the_batch_workload(oracle, ref):
         assert np.array_equal(u32(la), u32(lb)) and np.array_equal(u32(ga), u32(gb)), f"view {v} Linear/Guide"
 
 
+def test_port_equals_reference_on_the_headline_frames(oracle, ref, scenes):
+    """The measured configuration: seed 7 at 1920x1080, walk frames 0 and 40
+    (camera advanced by updateCamera from the seeded walk), sun shadows off
+    and on; trace + shade of three rows (300, 540, 800) bit-identical to the
+    reference harness."""
+    import workloads
+
+    s = scenes(7)
+    w, h = 1920, 1080
+    Ca, Cb = oracle.init_camera(s["P"], 7), ref.init_camera(s["P"], 7)
+    for frame in range(41):
+        I, dt = workloads.walk_input(frame, 7)
+        oracle.update_camera(Ca, I, s["P"], dt, w, h)
+        ref.update_camera(Cb, I, s["P"], dt, w, h)
+        assert np.array_equal(u32(Ca), u32(Cb)), frame
+        if frame not in (0, 40):
+            continue
+        for shadows in (0.0, 1.0):
+            C = Ca.copy()
+            C[22] = shadows
+            for y in (300, 540, 800):
+                ha = oracle.trace(s, C.copy(), w, h, y, y + 1)
+                hb = ref.trace(s, C.copy(), w, h, y, y + 1)
+                assert np.array_equal(u32(ha), u32(hb)), (frame, shadows, y)
+                la, ga = oracle.shade(s, C.copy(), ha, w, h, y, y + 1)
+                lb, gb = ref.shade(s, C.copy(), ha, w, h, y, y + 1)
+                assert np.array_equal(u32(la), u32(lb)) and np.array_equal(u32(ga), u32(gb)), (frame, shadows, y)
+
+
 def test_f64_rerun_close_to_f32(oracle, oracle64, scenes):
     """The FP64 instantiation runs the same formulas in double.
 
